@@ -1,0 +1,183 @@
+/*
+ * spinsim_b200 C ABI: the B200 (sm_100a) evaluation path of spinsim behind plain C entry points.
+ *
+ * The reference (alexander-tritt-monash/spinsim) is one Python module on numba; its evaluation path
+ * is Simulator(...).evaluate(...) -> Results(time, time_evolution, state, spin).  Each entry point
+ * below names the reference function it replaces (spinsim/__init__.py:line).
+ *
+ * Conventions
+ *  - Every function returns 0 (SPINSIM_OK) or a negative SPINSIM_ERR_* code; the message of the most
+ *    recent failure on the calling thread is available from spinsim_last_error().
+ *  - Array arguments named *_dev are device pointers (any allocator).  Complex arrays are interleaved
+ *    (re, im) doubles, numpy complex128 layout.  Output layouts match the reference's numpy outputs:
+ *      time[N] f64, time_evolution U[N][d][d] c128, state[N][d] c128, spin[N][3] f64.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  All work is stream-ordered; nothing
+ *    synchronises the host except spinsim_plan_create (module load).
+ *  - The library allocates no device memory on the evaluation path.  Scratch comes from the caller's
+ *    workspace, sized by the *_workspace_size queries (256-byte aligned start required).
+ */
+#ifndef SPINSIM_B200_H
+#define SPINSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPINSIM_OK 0
+#define SPINSIM_ERR_INVALID (-1)     /* bad argument (message says which) */
+#define SPINSIM_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define SPINSIM_ERR_LINK (-3)        /* nvJitLink / module load of a user field failed */
+#define SPINSIM_ERR_UNSUPPORTED (-4) /* method combination not built */
+#define SPINSIM_ERR_WORKSPACE (-5)   /* workspace too small or misaligned */
+
+/* Method enumerations: the values of the reference's IntegrationMethod (I:68-93) order and
+ * ExponentiationMethod.index (I:95-129). */
+#define SPINSIM_INTEGRATION_MAGNUS_CF4 0
+#define SPINSIM_INTEGRATION_EULER 1
+#define SPINSIM_INTEGRATION_HEUN 2
+#define SPINSIM_EXPONENTIATION_ANALYTIC 0
+#define SPINSIM_EXPONENTIATION_LIE_TROTTER 1
+#define SPINSIM_EXPONENTIATION_LIE_TROTTER_8 2
+#define SPINSIM_FIELD_USER 0  /* user get_field linked from LTO-IR (field_ltoir in plan_create) */
+#define SPINSIM_FIELD_TABLE 1 /* per-channel interpolation tables */
+#define SPINSIM_FIELD_TONES 2 /* per-channel bias + sum of sinusoids */
+#define SPINSIM_PRECISION_FP64 0
+#define SPINSIM_PRECISION_FP32_BULK 1
+
+/* Plan description: the compile-time specialisation of the reference's compile_time_evolver
+ * (I:453-991), i.e. Simulator.__init__ (I:375) minus the user callable. */
+typedef struct {
+    int32_t spin_dim;          /* 2 (SpinQuantumNumber.HALF), 3 (ONE), or 0 for a mixed batch */
+    int32_t integration;       /* SPINSIM_INTEGRATION_* */
+    int32_t expo_half;         /* exponentiation for dimension-2 instances */
+    int32_t expo_one;          /* exponentiation for dimension-3 instances */
+    int32_t rotating;          /* use_rotating_frame */
+    int32_t number_of_squares; /* number_of_squares (north_star: trotter_cutoff), >= 0 */
+    int32_t field_kind;        /* SPINSIM_FIELD_* */
+    int32_t precision;         /* SPINSIM_PRECISION_* */
+    int32_t threads_per_block; /* 0 = library default; else a multiple of 32, <= 1024 */
+    int32_t max_registers;     /* 0 = default; user-field plans pass it to the JIT linker */
+    int32_t lanes;             /* lanes per output interval: 0 = auto, else 1, 2, 4, 8, 16 or 32 */
+    int32_t reserved;
+} spinsim_plan_desc;
+
+/* One interpolation table: generate_interpolation_sampler's (time, amplitude, order,
+ * zero_boundary) (I:1941-2147).  time/amplitude are device pointers; size 0 = no table. */
+typedef struct {
+    const double* time;
+    const double* amplitude;
+    int64_t size;
+    int32_t order;
+    int32_t zero_boundary;
+} spinsim_table;
+
+/* Per-instance field (host struct whose pointers are device pointers).  Channel c (x, y, z, q,
+ * u1, u2, v1, v2) = bias[c] + gain[c] * source_c(t); source_c is tables[c] (FIELD_TABLE) or
+ * sum_k A_k sin(w_k t + phi_k) over tones[3 * (tone_start[c] + k) ...] as (w, A, phi)
+ * (FIELD_TONES).  FIELD_USER uses only params/n_params: the sweep_parameters of evaluate (I:993),
+ * handed to the user's get_field. */
+typedef struct {
+    const double* params;
+    int64_t n_params;
+    const spinsim_table* tables; /* device array [8] */
+    const double* tones;         /* device array */
+    int32_t tone_start[8];
+    int32_t tone_count[8];
+    double bias[8];
+    double gain[8];
+} spinsim_field;
+
+/* One evaluate() call inside a batch.  n_out and n_fine follow I:1025-1034 (use
+ * spinsim_normalise_steps).  Offsets place the instance in the flat output arrays: out_offset in
+ * intervals (time, spin), u_offset and state_offset in doubles. */
+typedef struct {
+    double t0;
+    double dt_int;
+    double dt_out;
+    int64_t n_out;
+    int64_t out_offset;
+    int64_t u_offset;
+    int64_t state_offset;
+    int32_t n_fine;
+    int32_t dim;
+    int32_t field;  /* index into the batch's field array */
+    int32_t reserved;
+    double psi0[6]; /* complex[dim] interleaved */
+} spinsim_instance;
+
+typedef struct spinsim_plan spinsim_plan;
+typedef struct spinsim_batch spinsim_batch;
+
+typedef struct {
+    int32_t registers_per_thread;
+    int32_t threads_per_block;
+    int32_t blocks_per_sm;  /* occupancy of the time-evolution kernel */
+    int32_t sm_count;
+    int32_t lanes;
+    int32_t linked;         /* 1 if the kernel came from nvJitLink (user field) */
+} spinsim_plan_info;
+
+/* Library version string. */
+const char* spinsim_version(void);
+
+/* Message of the last failure on this thread (copied into buf, NUL-terminated); returns its length. */
+int spinsim_last_error(char* buf, size_t n);
+
+/* Step normalisation of Simulator.evaluate, I:1025-1034: dt_int <- dt_out / round(max(dt_out/dt_int, 1)),
+ * N = int((t1 - t0) / dt_out), K = floor(dt_out / dt_int + 0.5).  *warned is set when the reference
+ * prints its non-integer-ratio warning (I:1027-1028). */
+int spinsim_normalise_steps(double t0, double t1, double dt_int, double dt_out, double* dt_int_out, int64_t* n_out,
+                            int32_t* n_fine, int32_t* warned);
+
+/* Build a plan: replaces compile_time_evolver (I:453-991).  For SPINSIM_FIELD_USER, field_ltoir holds
+ * the LTO-IR of `void spinsim_user_field(double t, double* sweep_parameters, int64_t n, double* field)`
+ * (field[0..8) pre-zeroed by the caller), which is linked into the kernel with nvJitLink; otherwise
+ * field_ltoir must be NULL.  Loads the module on the current device. */
+int spinsim_plan_create(const spinsim_plan_desc* desc, const void* field_ltoir, size_t field_ltoir_size,
+                        spinsim_plan** out);
+int spinsim_plan_destroy(spinsim_plan* plan);
+int spinsim_plan_get_info(const spinsim_plan* plan, spinsim_plan_info* info);
+
+/* Simulator.evaluate for one instance (I:993-1085): time evolution (get_time_evolution, I:855-896),
+ * state propagation (get_state, I:1089-1111, here a parallel scan) and, if spin_dev is non-NULL,
+ * the spin expectation (get_spin, I:899-959).  field is a host struct; psi0 a host complex[d] array. */
+size_t spinsim_evaluate_workspace_size(const spinsim_plan* plan, int64_t n_out);
+int spinsim_evaluate(const spinsim_plan* plan, const spinsim_field* field, double t0, double dt_int, double dt_out,
+                     int64_t n_out, const double* psi0, double* time_dev, double* u_dev, double* state_dev,
+                     double* spin_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
+
+/* get_time_evolution alone (I:855-896): writes time_dev[N] and u_dev[N][d][d]. */
+int spinsim_time_evolution(const spinsim_plan* plan, const spinsim_field* field, double t0, double dt_int,
+                           double dt_out, int64_t n_out, double* time_dev, double* u_dev, void* workspace_dev,
+                           size_t workspace_bytes, void* stream);
+
+/* get_state (I:1089-1111) as a parallel prefix scan, with get_spin (I:899-959) fused when spin_dev
+ * is non-NULL.  psi0 is a host complex[d] array. */
+size_t spinsim_state_workspace_size(int32_t dim, int64_t n_out);
+int spinsim_state(int32_t dim, const double* u_dev, int64_t n_out, const double* psi0, double* state_dev,
+                  double* spin_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
+
+/* get_spin alone (I:899-959; spin_calculator I:961-988): spin_dev[N][3] from state_dev[N][d]. */
+int spinsim_spin(int32_t dim, const double* state_dev, int64_t n_out, double* spin_dev, void* stream);
+
+/* Batched evaluation (no counterpart in the reference, which runs one evaluate() per sweep): many
+ * instances of possibly different spin, duration and step in one persistent launch.  prepare uploads
+ * the descriptors and the longest-first tile queue into the workspace (stream-ordered) and returns a
+ * handle; launch issues only kernel launches and a counter reset, so it can be captured into a CUDA
+ * graph and replayed.  Outputs are the flat arrays addressed by the instances' offsets. */
+size_t spinsim_batch_workspace_size(const spinsim_plan* plan, const spinsim_instance* instances,
+                                    int32_t n_instances, int32_t n_fields);
+int spinsim_batch_prepare(const spinsim_plan* plan, const spinsim_instance* instances, int32_t n_instances,
+                          const spinsim_field* fields, int32_t n_fields, void* workspace_dev,
+                          size_t workspace_bytes, void* stream, spinsim_batch** out);
+int spinsim_batch_launch(const spinsim_batch* batch, double* time_dev, double* u_dev, double* state_dev,
+                         double* spin_dev, void* stream);
+int spinsim_batch_destroy(spinsim_batch* batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPINSIM_B200_H */

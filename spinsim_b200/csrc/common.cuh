@@ -1,0 +1,191 @@
+// Shared device/host definitions for the spinsim sm_100a kernels.
+//
+// Layouts in HBM (the same as the reference's numpy outputs, spinsim/__init__.py:1040-1041, :1081):
+//   time[N]             float64
+//   U[N][d][d]          complex128, row-major per output interval (interleaved re, im)
+//   state[N][d]         complex128
+//   spin[N][3]          float64
+// A batch stores its instances back to back in the same flat arrays; every instance carries the
+// offsets of its first output interval.
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define SS_HD __host__ __device__ __forceinline__
+#define SS_D __device__ __forceinline__
+#else
+#define SS_HD inline
+#define SS_D inline
+#endif
+
+namespace spinsim {
+
+// ------------------------------------------------------------------ method enumerations
+// Values follow the reference's enums (IntegrationMethod I:68-93, ExponentiationMethod.index I:95-129).
+enum Integration : int { INTEG_CF4 = 0, INTEG_EULER = 1, INTEG_HEUN = 2 };
+enum Exponentiation : int { EXPO_ANALYTIC = 0, EXPO_LIE_TROTTER = 1, EXPO_LIE_TROTTER_8 = 2 };
+enum FieldKind : int { FIELD_USER = 0, FIELD_TABLE = 1, FIELD_TONES = 2 };
+enum Precision : int { PREC_FP64 = 0, PREC_FP32_BULK = 1 };
+
+constexpr int kMaxChannels = 8;  // x, y, z, q, u1, u2, v1, v2 (reference docs I:381-389)
+constexpr int kEvolveThreadsDefault = 128;  // time-evolution CTA size unless the plan asks otherwise
+constexpr int kEvolveThreadsMax = 256;      // __launch_bounds__ of the time-evolution kernels
+
+// ------------------------------------------------------------------ field descriptors
+// One interpolation table (the reference's generate_interpolation_sampler, I:1941-2147).
+struct TableChannel {
+    const double* time;       // [size], non-decreasing
+    const double* amplitude;  // [size]
+    int64_t size;             // 0 = no table on this channel
+    int32_t order;            // 0 zero-order hold, 1 linear, 3 cubic Hermite
+    int32_t zero_boundary;    // 1: zero outside [time[0], time[size-1]]; 0: hold the end values
+};
+
+// Per-instance field.  channel c = bias[c] + gain[c] * source_c(t), where source_c is the
+// channel's table (FIELD_TABLE) or its tone sum sum_k A_k sin(w_k t + phi_k) (FIELD_TONES).
+// FIELD_USER ignores everything but params/n_params, which go to the linked get_field().
+struct FieldDesc {
+    const double* params;          // sweep parameters for a user get_field (device)
+    int64_t n_params;
+    const TableChannel* tables;    // [kMaxChannels] (FIELD_TABLE)
+    const double* tones;           // FIELD_TONES: (w, A, phi) triples, channel after channel
+    int32_t tone_start[kMaxChannels];
+    int32_t tone_count[kMaxChannels];
+    double bias[kMaxChannels];
+    double gain[kMaxChannels];
+};
+
+// ------------------------------------------------------------------ work description
+// One simulated instance (one evaluate() call of the reference).
+struct Instance {
+    double t0;            // time_start
+    double dt_int;        // normalised integration step (I:1025-1026)
+    double dt_out;        // time_step_output
+    int64_t n_out;        // N = int((t1 - t0) / dt_out)  (I:1034)
+    int64_t out_offset;   // first output interval of this instance in time[] and spin[]
+    int64_t u_offset;     // first double of this instance in U[] (out_offset * 2 d^2 when all d agree)
+    int64_t state_offset; // first double of this instance in state[]
+    int32_t n_fine;       // K = floor(dt_out / dt_int + 0.5)  (I:832)
+    int32_t dim;          // 2 or 3
+    int32_t field;        // index into the FieldDesc array
+    int32_t pad;
+    double psi0[6];       // initial state, complex[dim] interleaved
+};
+
+// A tile is a warp's unit of work: up to 32 / lanes consecutive output intervals of one instance.
+struct Tile {
+    int32_t instance;
+    int32_t count;      // intervals in this tile
+    int64_t first;      // first output interval (relative to the instance)
+};
+
+// Static configuration of one time-evolution launch (identical for every instance in it).
+struct MethodConfig {
+    int32_t integration;    // Integration
+    int32_t expo_half;      // Exponentiation used for dim 2 instances
+    int32_t expo_one;       // Exponentiation used for dim 3 instances
+    int32_t rotating;       // use_rotating_frame
+    int32_t hypercubes;     // ceil(number_of_squares / 2), >= 0  (I:1547-1549)
+    int32_t lanes;          // lanes sharing one output interval (1, 2, 4, 8, 16, 32)
+    double precision;       // 4 ** hypercubes  (I:1550)
+};
+
+struct EvolveArgs {
+    MethodConfig m;
+    const Instance* instances;
+    const FieldDesc* fields;
+    const Tile* tiles;       // null: single instance, implicit tiles of 32 / lanes intervals
+    int64_t n_tiles;
+    int32_t* tile_counter;   // null: one tile per warp of the grid, no queue
+    double* time;            // [sum N]
+    double* u;               // complex [sum N * d * d]; instance i starts at u_offset doubles
+};
+
+// ------------------------------------------------------------------ complex helpers (FP64)
+struct c64 {
+    double re, im;
+};
+SS_HD c64 mk(double r, double i) { return c64{r, i}; }
+SS_HD c64 operator+(c64 a, c64 b) { return c64{a.re + b.re, a.im + b.im}; }
+SS_HD c64 operator-(c64 a, c64 b) { return c64{a.re - b.re, a.im - b.im}; }
+SS_HD c64 operator*(c64 a, c64 b) { return c64{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+SS_HD c64 operator*(double s, c64 a) { return c64{s * a.re, s * a.im}; }
+SS_HD c64 conj(c64 a) { return c64{a.re, -a.im}; }
+// a * b + c
+SS_HD c64 cfma(c64 a, c64 b, c64 c) {
+#ifdef __CUDA_ARCH__
+    return c64{fma(a.re, b.re, fma(-a.im, b.im, c.re)), fma(a.re, b.im, fma(a.im, b.re, c.im))};
+#else
+    return c64{a.re * b.re - a.im * b.im + c.re, a.re * b.im + a.im * b.re + c.im};
+#endif
+}
+
+template <int D>
+struct Mat {
+    c64 a[D][D];
+};
+
+template <int D>
+SS_HD void set_identity(Mat<D>& m) {
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) m.a[i][j] = c64{i == j ? 1.0 : 0.0, 0.0};
+}
+
+// matrix_multiply (I:1594-1600, I:1722-1734): out = l r
+template <int D>
+SS_HD Mat<D> matmul(const Mat<D>& l, const Mat<D>& r) {
+    Mat<D> o;
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            c64 acc = l.a[i][0] * r.a[0][j];
+#pragma unroll
+            for (int k = 1; k < D; k++) acc = cfma(l.a[i][k], r.a[k][j], acc);
+            o.a[i][j] = acc;
+        }
+    return o;
+}
+
+// matrix_square_m1 (I:1602-1608, I:1736-1748): (2 + A) A, the k == i term grouped as (2 + A_ii) A_ij
+template <int D>
+SS_HD Mat<D> square_m1(const Mat<D>& m) {
+    Mat<D> o;
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            c64 acc = c64{0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                if (k == i) {
+                    c64 two_plus = c64{2.0 + m.a[i][i].re, m.a[i][i].im};
+                    acc = (k == 0) ? two_plus * m.a[i][j] : cfma(two_plus, m.a[i][j], acc);
+                } else {
+                    acc = (k == 0) ? m.a[i][k] * m.a[k][j] : cfma(m.a[i][k], m.a[k][j], acc);
+                }
+            }
+            o.a[i][j] = acc;
+        }
+    return o;
+}
+
+// matrix_multiply_m1 (I:1610-1616, I:1750-1762): (l + r) + l r
+template <int D>
+SS_HD Mat<D> multiply_m1(const Mat<D>& l, const Mat<D>& r) {
+    Mat<D> o;
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            c64 acc = l.a[i][0] * r.a[0][j];
+#pragma unroll
+            for (int k = 1; k < D; k++) acc = cfma(l.a[i][k], r.a[k][j], acc);
+            o.a[i][j] = (l.a[i][j] + r.a[i][j]) + acc;
+        }
+    return o;
+}
+
+}  // namespace spinsim
