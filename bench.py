@@ -1,0 +1,443 @@
+"""Benchmark: steps/s of the batched FP32-bulk form vs the plain FP64 form on B200.
+
+Workload (one "step" = one pass of the hot path over the whole batch): 1024 instances, 70% spin half
+(analytic exponential) / 30% spin one (Lie-Trotter, 24 squarings), durations log-uniform in
+[10 us, 10 ms], dt_int 10 ns, dt_out 1 us, Magnus CF4, rotating frame, field = 8 tones per axis
+(frequency U[0, 1 MHz], amplitude U[0, 2pi 10 kHz], phase U[0, 2pi)) from a per-instance seed,
+q = 0; all instances in one persistent launch replayed from a CUDA graph, followed by the FP64
+prefix scan (state) with the spin expectation fused.  Synthetic inputs (seeded).
+
+The headline ``value`` is the FP32-bulk steps/s with inputs resident in HBM; ``plain_fp64`` is the
+plain FP64 form on the same batch, ``state_err`` the final-state error of FP32-bulk against FP64.
+``e2e`` repeats the measurement through the public API with host inputs and host outputs
+(descriptors and tone tables copied in, time / time_evolution / state / spin copied out, every
+step).  ``--impl reference`` times the reference's CPU algorithm (the oracle restatement, all host
+threads) on a bounded sample of the same workload.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU: torchrun --nproc-per-node N bench.py --gpus N (weak scaling: every rank runs its own
+batch of the same shape from its own seeds; no collective on the data path).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+
+METRIC = "steps/s batched FP32-bulk vs plain FP64 at state err<=1e-6; p50/p99 latency"
+N_INSTANCES = 1024
+TAU = 2 * np.pi
+
+
+# ------------------------------------------------------------------------------------ workload
+def workload(seed_base=0, n=N_INSTANCES):
+    """Instance specs: (spin_dim, duration, tone parameter vector)."""
+    rng = np.random.default_rng(3 + 7919 * seed_base)
+    specs = []
+    for k in range(n):
+        dim = 2 if rng.uniform() < 0.7 else 3
+        dur = float(np.exp(rng.uniform(np.log(10e-6), np.log(10e-3))))
+        p = np.zeros(4 + 72)
+        r = np.random.default_rng(10_000 + k + 1_000_003 * seed_base)
+        for axis in range(3):
+            for tone in range(8):
+                b = 4 + 24 * axis + 3 * tone
+                p[b] = TAU * r.uniform(0.0, 1e6)
+                p[b + 1] = r.uniform(0.0, TAU * 10e3)
+                p[b + 2] = r.uniform(0.0, TAU)
+        specs.append((dim, dur, p))
+    return specs
+
+
+def tone_field(ss, p):
+    tones = {a: np.array([(p[4 + 24 * a + 3 * j], p[5 + 24 * a + 3 * j], p[6 + 24 * a + 3 * j]) for j in range(8)])
+             for a in range(3)}
+    return ss.ToneField(tones, bias=list(p[:4]))
+
+
+def instances(ss, specs):
+    from spinsim_b200.batch import Instance
+    out = []
+    for dim, dur, p in specs:
+        spin = ss.SpinQuantumNumber.HALF if dim == 2 else ss.SpinQuantumNumber.ONE
+        psi0 = spin.plus_z if dim == 2 else spin.plus_x
+        out.append(Instance(spin, 0.0, dur, 10e-9, 1e-6, psi0, sweep_parameters=p, field=tone_field(ss, p)))
+    return out
+
+
+# Algorithmic work per integration step, counted from the kernels' arithmetic (a fused multiply-add
+# is 2 flops; sin, cos, sqrt and division count 1 each).  See DESIGN.md, "Work per step".
+FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
+FLOPS_BULK = {2: {"fp64": 467, "fp32": 82}, 3: {"fp64": 467, "fp32": 82}}
+
+
+def algorithmic_flops(specs, form):
+    total64 = total32 = 0.0
+    for dim, dur, _ in specs:
+        n = int(dur / 1e-6)
+        steps = n * 100
+        if form == "fp64":
+            total64 += steps * FLOPS_FP64_PLAIN[dim]
+        else:
+            total64 += steps * FLOPS_BULK[dim]["fp64"]
+            total32 += steps * FLOPS_BULK[dim]["fp32"]
+    return total64, total32
+
+
+# ------------------------------------------------------------------------------------ helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks_from_file():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier_max(value, world):
+    """Max over ranks of a float (device timing); identity on one rank."""
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------ CPU baseline
+def cpu_sample(specs, seconds_target=8.0, n_threads=0):
+    """Time the oracle (the reference's algorithm restated in C, all host threads) on a bounded sample
+    of the workload: the first intervals of every instance, grown until it takes ~seconds_target."""
+    from oracle import oracle as O
+    fields = []
+    for dim, dur, p in specs:
+        fields.append((dim, p, int(dur / 1e-6)))
+    field = O.Field(8)
+
+    def run(frac):
+        steps = 0
+        t0 = time.perf_counter()
+        for dim, p, n in fields:
+            cnt = max(1, int(n * frac)) if n else 0
+            if cnt == 0:
+                continue
+            O.time_evolution(dim, field, p, 0.0, 10e-9, 1e-6, n, first=0, count=cnt, n_threads=n_threads)
+            steps += cnt * 100
+        return steps, time.perf_counter() - t0
+
+    frac = 0.002
+    steps, el = run(frac)
+    while el < seconds_target / 4 and frac < 1.0:
+        frac = min(1.0, frac * max(2.0, seconds_target / max(el, 1e-3) / 2))
+        steps, el = run(frac)
+    return steps, el, frac
+
+
+# ------------------------------------------------------------------------------------ our arm
+def bench_ours(args, world, rank):
+    import torch
+    import spinsim_b200 as ss
+    from spinsim_b200.batch import Batch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    specs = workload(seed_base=rank)
+    insts = instances(ss, specs)
+    total_steps = sum(int(d / 1e-6) * 100 for _, d, _ in specs)
+    plans = {}
+    bulk = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+    plain = Batch(insts, precision=ss.Precision.FP64, plan_cache=plans)
+    assert bulk.total_steps == total_steps
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
+
+    def timed(batch, k, evolve_only=False):
+        for _ in range(args.warmup):
+            batch.run(with_state=not evolve_only)
+        torch.cuda.synchronize()
+        times = []
+        stream = torch.cuda.current_stream(dev)
+        for _ in range(k):
+            flush.zero_()
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            if evolve_only:
+                batch.run(with_state=False)
+            else:
+                batch.replay()
+            e.record(stream)
+            times.append((s, e))
+        torch.cuda.synchronize()
+        return [s.elapsed_time(e) / 1e3 for s, e in times]
+
+    bulk.capture()
+    plain.capture()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        t_bulk = timed(bulk, args.steps)
+    t_bulk_total = barrier_max(sum(t_bulk), world)
+    t_plain = timed(plain, max(1, args.steps // 3))
+    t_plain_total = barrier_max(sum(t_plain), world) * args.steps / len(t_plain)
+
+    # dominant kernel alone (time evolution), same stream, CUDA events
+    t_evolve = timed(bulk, max(2, args.steps // 2), evolve_only=True)
+    t_evolve_plain = timed(plain, 1, evolve_only=True)
+
+    # accuracy of FP32-bulk against FP64 on this batch
+    bulk.replay()
+    plain.replay()
+    torch.cuda.synchronize()
+    fb, fp = bulk.final_states(), plain.final_states()
+    errs = np.array([np.abs(a - b).max() if a.size else 0.0 for a, b in zip(fb, fp)])
+
+    # end to end through the public API with host buffers
+    e2e_times, h2d, d2h = [], 0, 0
+    pinned = None
+    for it in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+        b.run()
+        outs = [b.time, b.u, b.state, b.spin]
+        if pinned is None:
+            pinned = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
+        for hst, o in zip(pinned, outs):
+            hst.copy_(o, non_blocking=True)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        if it >= args.warmup:
+            e2e_times.append(el)
+        if it == 0:
+            d2h = sum(o.numel() * o.element_size() for o in outs)
+            h2d = b.h2d_bytes
+        del b
+    e2e_total = barrier_max(sum(e2e_times), world)
+
+    info = bulk.plan_info()
+    peaks = peaks_from_file()
+    fp64_flops, fp32_flops = algorithmic_flops(specs, "bulk")
+    evolve_s = float(np.mean(t_evolve))
+    fp64_peak = measured_fp64_peak()
+    achieved = fp64_flops / evolve_s / 1e12
+    fp64_plain_flops, _ = algorithmic_flops(specs, "fp64")
+    value = world * total_steps * args.steps / t_bulk_total
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_bulk_total / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32+fp64",
+        "data": "synthetic (seeded tone fields)",
+        "config": {"workload": "uneven batch: 1024 instances, 70% spin-1/2 analytic / 30% spin-1 Lie-Trotter(24), "
+                               "durations log-uniform 10us-10ms, dt_int 10ns, dt_out 1us, 8 tones per axis, "
+                               "Magnus CF4, rotating frame, one persistent launch (CUDA graph)",
+                   "instances_per_gpu": len(specs), "integration_steps_per_gpu": total_steps,
+                   "l2": "256 MB buffer written between timed steps", "lanes": info["lanes"],
+                   "threads_per_block": info["threads_per_block"], "registers": info["registers_per_thread"]},
+        "latency_ms": {"p50": 1e3 * float(np.percentile(t_bulk, 50)), "p99": 1e3 * float(np.percentile(t_bulk, 99))},
+        "plain_fp64": {"value": world * total_steps * args.steps / t_plain_total, "unit": "steps/s",
+                       "ms_per_step": 1e3 * t_plain_total / args.steps,
+                       "evolve_kernel_ms": 1e3 * float(np.mean(t_evolve_plain)),
+                       "fp64_tflops": fp64_plain_flops / float(np.mean(t_evolve_plain)) / 1e12},
+        "speedup_vs_fp64": t_plain_total / t_bulk_total,
+        "state_err": {"max": float(errs.max()), "p50": float(np.median(errs)), "p99": float(np.percentile(errs, 99)),
+                      "tolerance": 1e-6, "vs": "plain FP64 form, final state state[N-1] per instance"},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak["tflops"], "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak["tflops"], "traffic": None,
+                     "kernel": "spinsim::evolve_kernel (FP32-bulk, mixed dims, tones)",
+                     "peak_source": fp64_peak["source"],
+                     "fp32_achieved": fp32_flops / evolve_s / 1e12,
+                     "kernel_ms": 1e3 * evolve_s},
+        "gpu_launches": 7 * args.steps,
+        "clocks": clocks.summary(),
+        "e2e": {"value": world * total_steps * len(e2e_times) / e2e_total, "unit": "steps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+    }
+    if peaks:
+        out["hbm_peak_gbs"] = peaks.get("hbm_gbs")
+    return out, specs
+
+
+_PEAK = {}
+
+
+def measured_fp64_peak():
+    """FP64 FMA throughput of this GPU measured in-run (dependent-chain-free DFMA loop)."""
+    if "fp64" not in _PEAK:
+        import torch
+        import spinsim_b200 as ss
+        lib = ss._lib.load()
+        flops = ss._lib.c_dbl()
+        dev = torch.cuda.current_device()
+        best = 0.0
+        stream = torch.cuda.current_stream().cuda_stream
+        for _ in range(3):
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record()
+            ss._lib.check(lib.spinsim_fma_peak(0, ss._lib.ctypes.byref(flops), stream))
+            e.record()
+            torch.cuda.synchronize()
+            best = max(best, flops.value / (s.elapsed_time(e) / 1e3) / 1e12)
+        _PEAK["fp64"] = {"tflops": best, "source": f"measured in-run on GPU {dev} (FP64 FMA loop)"}
+    return _PEAK["fp64"]
+
+
+# ------------------------------------------------------------------------------------ reference arm
+def bench_reference(args, world, rank):
+    from oracle import oracle as O
+    specs = workload(seed_base=0)
+    O.lib()
+    threads = O.max_threads()
+    times, steps_list = [], []
+    _, _, frac = cpu_sample(specs, seconds_target=min(8.0, 120.0 / max(1, args.steps + args.warmup)))
+    field = O.Field(8)
+    for it in range(args.warmup + args.steps):
+        steps = 0
+        t0 = time.perf_counter()
+        for dim, dur, p in specs:
+            n = int(dur / 1e-6)
+            cnt = max(1, int(n * frac)) if n else 0
+            if cnt:
+                O.time_evolution(dim, field, p, 0.0, 10e-9, 1e-6, n, first=0, count=cnt)
+                steps += cnt * 100
+        el = time.perf_counter() - t0
+        if it >= args.warmup:
+            times.append(el)
+            steps_list.append(steps)
+    value = sum(steps_list) / sum(times)
+    sample = (f"first {frac:.4f} of the output intervals of each of the {len(specs)} instances "
+              f"({steps_list[0]} integration steps per step)")
+    return {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tone fields)",
+        "impl": "reference",
+        "config": {"workload": "uneven batch: 1024 instances (bounded sample per step)", "threads": threads},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(bench_reference(args, world, rank)), flush=True)
+        return
+    import torch
+    if not torch.cuda.is_available():
+        print(json.dumps({"metric": METRIC, "unavailable": "no CUDA device"}))
+        return
+    torch.cuda.set_device(local)
+    out, specs = bench_ours(args, world, rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        steps, el, frac = cpu_sample(specs, seconds_target=10.0)
+        out["cpu_baseline"] = {"value": steps / el, "unit": "steps/s", "cores": O.max_threads(), "kind": "port",
+                               "sample": f"oracle (reference algorithm in C, OpenMP) on the first {frac:.4f} of "
+                                         f"the output intervals of every instance: {steps} integration steps"}
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

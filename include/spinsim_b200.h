@@ -177,6 +177,11 @@ int spinsim_batch_launch(const spinsim_batch* batch, double* time_dev, double* u
                          double* spin_dev, void* stream);
 int spinsim_batch_destroy(spinsim_batch* batch);
 
+/* Diagnostics (no counterpart in the reference): one launch of an FMA-throughput loop that fills the
+ * device (precision 0: FP64, 1: FP32).  *flops receives the operations it performs; time the launch
+ * with events on `stream` to get the pipe's peak rate, the denominator of the kernels' roofline. */
+int spinsim_fma_peak(int32_t precision, double* flops, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

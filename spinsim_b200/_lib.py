@@ -85,6 +85,7 @@ _SIGNATURES = [
       ctypes.POINTER(c_vp)]),
     ("spinsim_batch_launch", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("spinsim_batch_destroy", ctypes.c_int, [c_vp]),
+    ("spinsim_fma_peak", ctypes.c_int, [c_i32, ctypes.POINTER(c_dbl), c_vp]),
 ]
 
 EXPORTED = [name for name, _, _ in _SIGNATURES]

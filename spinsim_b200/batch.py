@@ -127,12 +127,14 @@ class Batch:
             u_off += 2 * d * d * n_out
             st_off += 2 * d * n_out
             self.total_steps += n_out * n_fine
-            if get_field is None:
-                f, kp = inst.field.device_struct(dev)
-                keep += kp
-                fields.append(f)
-            else:
+            if get_field is not None:
                 params_host.append(np.asarray(inst.sweep_parameters, np.float64).reshape(-1))
+        self.h2d_bytes = 0
+        if get_field is None:
+            from .fields import pack_fields
+            fields, kp, nbytes = pack_fields([i.field for i in self.instances], dev)
+            keep += kp
+            self.h2d_bytes += nbytes
         if get_field is not None:
             sizes = [max(1, p.size) for p in params_host]
             flat = np.zeros(sum(sizes))
@@ -141,6 +143,7 @@ class Batch:
                 flat[o:o + p.size] = p
             params_dev = torch.from_numpy(flat).to(dev)
             keep.append(params_dev)
+            self.h2d_bytes += flat.nbytes
             for p, o in zip(params_host, offs):
                 f = _lib.Field()
                 f.params = params_dev.data_ptr() + 8 * int(o)
@@ -148,6 +151,7 @@ class Batch:
                 fields.append(f)
         self.n_intervals = out_off
         fields_arr = (_lib.Field * n)(*fields)
+        self.h2d_bytes += ctypes.sizeof(insts) + ctypes.sizeof(fields_arr)
         self._insts, self._fields, self._keep = insts, fields_arr, keep
         self.time = torch.empty(max(1, out_off), dtype=torch.float64, device=dev)
         self.u = torch.empty(max(1, u_off // 2), dtype=torch.complex128, device=dev)

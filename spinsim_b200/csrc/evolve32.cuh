@@ -1,14 +1,433 @@
-// FP32-bulk time evolution of one output interval (see interval32 below).
+// FP32-bulk time evolution of one output interval (Magnus CF4, batched form).
+//
+// Precision split (errors are stated against the FP64 path, which matches the reference):
+//   FP64  sample times, the rotating-frame phase (a phasor recurrence per interval), field samples
+//         (tones by FP64 phasor recurrences), the frame transform, the CF4 generator combinations,
+//         and the product of steps within the output interval.
+//   FP32  the per-step exponentials in residual form exp(A) - 1, and the product of the two CF4
+//         exponentials of a step.  Only quantities that are recomputed every step are rounded to
+//         FP32, so FP32 rounding errors do not correlate from step to step; constants and
+//         recurrences are never held in FP32.
+//
+// Exponentials.  Spin half: the exact SU(2) exponential exp(-i g.sigma/2) - 1 from even power
+// series in r^2 = |g|^2 (no square root or division) for r <= 1/2, sincos otherwise.  Spin one with
+// no quadratic shift in the step: the same SU(2) element mapped to its spin-one representation
+// D1 (the homomorphism exp(-i g.J1) = D1(exp(-i g.sigma/2))); the step product and the interval
+// product are then kept as SU(2) elements (2x2), mapped to 3x3 once per output interval.  Spin one
+// with a quadratic shift: a Taylor series of exp(A) - 1 in A = -i(x Jx + y Jy + z Jz + q Q).  The
+// reference's Lie-Trotter product approximates these exponentials to about
+// |[A, B]| / (2 * 4^h) per exponential (h = number of squarings / 2).
 #pragma once
 #include "common.cuh"
 #include "evolve64.cuh"
 
 namespace spinsim {
 
+struct c32 {
+    float re, im;
+};
+SS_D c32 operator+(c32 a, c32 b) { return c32{a.re + b.re, a.im + b.im}; }
+SS_D c32 operator-(c32 a, c32 b) { return c32{a.re - b.re, a.im - b.im}; }
+SS_D c32 operator*(c32 a, c32 b) { return c32{fmaf(a.re, b.re, -a.im * b.im), fmaf(a.re, b.im, a.im * b.re)}; }
+SS_D c32 operator*(float s, c32 a) { return c32{s * a.re, s * a.im}; }
+SS_D c32 conjf(c32 a) { return c32{a.re, -a.im}; }
+SS_D c32 cfmaf(c32 a, c32 b, c32 c) {
+    return c32{fmaf(a.re, b.re, fmaf(-a.im, b.im, c.re)), fmaf(a.re, b.im, fmaf(a.im, b.re, c.im))};
+}
+
+template <int D>
+struct Mat32 {
+    c32 a[D][D];
+};
+
+// SU(2) element in residual form: alpha = 1 + am1, U = [[alpha, -conj(beta)], [beta, conj(alpha)]].
+struct Su2f {
+    c32 am1, beta;
+};
+struct Su2d {
+    c64 am1, beta;
+};
+
+// exp(-i (x sigma_x + y sigma_y + z sigma_z) / 2) - 1 as (alpha - 1, beta); the reference's analytic
+// spin-half exponential (I:1618-1642) is the same element.
+SS_D Su2f su2_exp(float x, float y, float z) {
+    const float r2 = fmaf(x, x, fmaf(y, y, z * z));
+    float c, s;  // c = cos(r/2) - 1, s = sin(r/2) / r
+    if (r2 <= 0.25f) {
+        c = r2 * (-0.125f + r2 * (1.0f / 384.0f + r2 * (-1.0f / 46080.0f + r2 * (1.0f / 10321920.0f -
+                                                                            r2 * (1.0f / 3715891200.0f)))));
+        s = 0.5f + r2 * (-1.0f / 48.0f + r2 * (1.0f / 3840.0f + r2 * (-1.0f / 645120.0f + r2 * (1.0f / 185794560.0f))));
+    } else {
+        const float r = sqrtf(r2);
+        float s4, c4;
+        sincosf(0.25f * r, &s4, &c4);
+        c = -2.0f * s4 * s4;
+        s = 2.0f * s4 * c4 / r;
+    }
+    Su2f e;
+    e.am1 = c32{c, -z * s};
+    e.beta = c32{y * s, -x * s};
+    return e;
+}
+
+// b * a (a first) in residual form
+SS_D Su2f su2_mul(const Su2f& b, const Su2f& a) {
+    // alpha = ab_a - conj(bb) ba; beta = bb aa + conj(ab) ba
+    Su2f o;
+    const c32 cross = conjf(b.beta) * a.beta;
+    o.am1 = (b.am1 * a.am1 + (b.am1 + a.am1)) - cross;
+    o.beta = (b.beta * a.am1 + b.beta) + (conjf(b.am1) * a.beta + a.beta);
+    return o;
+}
+
+SS_D Mat32<2> su2_mat_m1(const Su2f& e) {
+    Mat32<2> m;
+    m.a[0][0] = e.am1;
+    m.a[1][0] = e.beta;
+    m.a[0][1] = c32{-e.beta.re, e.beta.im};  // -conj(beta)
+    m.a[1][1] = conjf(e.am1);
+    return m;
+}
+
+// Spin-one representation of an FP64 SU(2) element (full matrix, not residual).
+SS_D Mat<3> su2_to_spin_one(const c64& alpha, const c64& beta) {
+    constexpr double r2 = 1.4142135623730951;
+    Mat<3> m;
+    const c64 ac = conj(alpha), bc = conj(beta);
+    m.a[0][0] = alpha * alpha;
+    m.a[1][0] = r2 * (alpha * beta);
+    m.a[2][0] = beta * beta;
+    m.a[0][1] = (-r2) * (alpha * bc);
+    m.a[1][1] = c64{alpha.re * alpha.re + alpha.im * alpha.im - beta.re * beta.re - beta.im * beta.im, 0.0};
+    m.a[2][1] = r2 * (ac * beta);
+    m.a[0][2] = bc * bc;
+    m.a[1][2] = (-r2) * (ac * bc);
+    m.a[2][2] = ac * ac;
+    return m;
+}
+
+// exp(A) - 1 for A = -i H, H = x Jx + y Jy + z Jz + q Q (spin one, Q = diag(1, -2, 1) / 3), by a
+// Taylor series to A^6 / 6! on A scaled to norm <= 1/32 (truncation below 2e-13 relative),
+// followed by residual squarings (E - 1 -> 2 (E - 1) + (E - 1)^2) when it was scaled.
+SS_D Mat32<3> spin_one_exp_m1(float x, float y, float z, float q) {
+    constexpr float ir2 = 0.70710678118654752f;
+    const float pr = x * ir2, pi = y * ir2;
+    const float h0 = z + q * (1.0f / 3.0f), h1 = -q * (2.0f / 3.0f), h2 = -z + q * (1.0f / 3.0f);
+    int squarings = 0;
+    float scale = 1.0f;
+    const float norm = fabsf(x) + fabsf(y) + fabsf(z) + fabsf(q);
+    while (norm * scale > 0.03125f && squarings < 40) {
+        scale *= 0.5f;
+        squarings++;
+    }
+    // A = -i H (scaled); H[1][0] = H[2][1] = (x + i y) / sqrt2, H[0][1] = H[1][2] = (x - i y) / sqrt2
+    Mat32<3> A;
+    A.a[0][0] = c32{0.0f, -h0 * scale};
+    A.a[1][1] = c32{0.0f, -h1 * scale};
+    A.a[2][2] = c32{0.0f, -h2 * scale};
+    A.a[1][0] = c32{pi * scale, -pr * scale};
+    A.a[2][1] = A.a[1][0];
+    A.a[0][1] = c32{-pi * scale, -pr * scale};
+    A.a[1][2] = A.a[0][1];
+    A.a[2][0] = c32{0.0f, 0.0f};
+    A.a[0][2] = c32{0.0f, 0.0f};
+    // R_6 = A / 6;  R_k = (A + A R_{k+1}) / k for k = 5 .. 1;  E - 1 = R_1
+    const float inv[6] = {1.0f, 0.5f, 1.0f / 3.0f, 0.25f, 0.2f, 1.0f / 6.0f};
+    Mat32<3> R;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) R.a[i][j] = inv[5] * A.a[i][j];
+#pragma unroll
+    for (int k = 5; k >= 1; k--) {
+        Mat32<3> N;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                c32 acc = A.a[i][j];
+#pragma unroll
+                for (int l = 0; l < 3; l++) acc = cfmaf(A.a[i][l], R.a[l][j], acc);
+                N.a[i][j] = inv[k - 1] * acc;
+            }
+        R = N;
+    }
+    for (int s = 0; s < squarings; s++) {
+        Mat32<3> N;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                c32 acc = c32{2.0f * R.a[i][j].re, 2.0f * R.a[i][j].im};
+#pragma unroll
+                for (int l = 0; l < 3; l++) acc = cfmaf(R.a[i][l], R.a[l][j], acc);
+                N.a[i][j] = acc;
+            }
+        R = N;
+    }
+    return R;
+}
+
+template <int D>
+SS_D Mat32<D> mul_m1_f(const Mat32<D>& l, const Mat32<D>& r) {  // (l + r) + l r
+    Mat32<D> o;
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            c32 acc = l.a[i][j] + r.a[i][j];
+#pragma unroll
+            for (int k = 0; k < D; k++) acc = cfmaf(l.a[i][k], r.a[k][j], acc);
+            o.a[i][j] = acc;
+        }
+    return o;
+}
+
+// U <- U + D U with D in FP32 (converted once) and U in FP64.
+template <int D>
+SS_D void apply_m1(Mat<D>& u, const Mat32<D>& dm) {
+    c64 d[D][D];
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int k = 0; k < D; k++) d[i][k] = c64{(double)dm.a[i][k].re, (double)dm.a[i][k].im};
+    Mat<D> o;
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            c64 acc = u.a[i][j];
+#pragma unroll
+            for (int k = 0; k < D; k++) acc = cfma(d[i][k], u.a[k][j], acc);
+            o.a[i][j] = acc;
+        }
+    u = o;
+}
+
+// SU(2) product in FP64: P <- (1 + E) P, with E an FP32 residual element.
+SS_D void su2_apply(Su2d& p, const Su2f& e) {
+    const c64 am1 = c64{(double)e.am1.re, (double)e.am1.im};
+    const c64 b = c64{(double)e.beta.re, (double)e.beta.im};
+    // alpha' = alpha_e alpha - conj(beta_e) beta ; beta' = beta_e alpha + conj(alpha_e) beta
+    const c64 alpha = c64{1.0 + p.am1.re, p.am1.im};
+    const c64 na = cfma(am1, alpha, p.am1) - conj(b) * p.beta;  // (alpha - 1) + am1 alpha - conj(b) beta
+    const c64 nb = cfma(b, alpha, cfma(conj(am1), p.beta, p.beta));
+    p.am1 = na;
+    p.beta = nb;
+}
+
+// ---------------------------------------------------------------------------------- tone recurrences
+constexpr int kBulkTones = 8;  // tones per channel (x, y, z) carried as FP64 phasors in registers
+
+// Per-instance tone constants, shared by the warp (all its lanes work on one instance).
+struct ToneConst {
+    double rot_re, rot_im;  // exp(i w dt)
+    double off_re, off_im;  // exp(i w a_lo)
+    double amp;             // gain * A
+};
+
 template <int D, int INTEG, int EXPO, int FIELD>
 SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDesc& f, int64_t index, bool active,
                      int lane_in_group, double* time_out, double* u_out) {
-    static_assert(D < 0, "FP32-bulk kernels are not built yet");
+    static_assert(INTEG == INTEG_CF4, "the FP32-bulk form is built for Magnus CF4");
+    static_assert(EXPO != EXPO_LIE_TROTTER_8, "the FP32-bulk form has no eight-generator exponential");
+    constexpr int L = (D == 2) ? 3 : 4;
+    constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
+    const int lanes = m.lanes;
+    const double dt = inst.dt_int, dt_out = inst.dt_out;
+    const double t_c = inst.t0 + dt_out * (double)index;
+    double s0[8], s1[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        s0[k] = 0.0;
+        s1[k] = 0.0;
+    }
+    double rw = 0.0;
+    if (active && m.rotating) {
+        sample_field<FIELD, L>(f, t_c + dt_out / 2, s0);
+        rw = s0[2];
+        if (D == 2) rw /= 2;
+    }
+    const int K = active ? inst.n_fine : 0;
+    const int j0 = (int)(((int64_t)K * lane_in_group) / lanes);
+    const int j1 = (int)(((int64_t)K * (lane_in_group + 1)) / lanes);
+    double t_fine = t_c;
+    for (int j = 0; j < j0; j++) t_fine += dt;
+
+    const double a_lo = 0.5 * dt * (1.0 - 1.0 / kSqrt3);
+    const double a_hi = 0.5 * dt * (1.0 + 1.0 / kSqrt3);
+    const double w0 = (1.5 + kSqrt3) / 6.0, w1 = (1.5 - kSqrt3) / 6.0;
+    const double c0 = dt * w0, c1 = dt * w1;
+
+    // Frame phasor W(t) = exp(-i P rw (t - t_c)) by an FP64 recurrence, anchored at this lane's start.
+    c64 W = c64{1.0, 0.0}, Wrot = c64{1.0, 0.0}, Woff = c64{1.0, 0.0};
+    if (m.rotating && K > 0) {
+        sincos(-(double)P * rw * (t_fine - t_c), &W.im, &W.re);
+        sincos(-(double)P * rw * dt, &Wrot.im, &Wrot.re);
+        sincos(-(double)P * rw * a_lo, &Woff.im, &Woff.re);
+    }
+
+    // Tone phasors z = exp(i (w t + phi)) at the step start, FP64 (FIELD_TONES only).
+    constexpr int NT = (FIELD == FIELD_TONES) ? 3 * kBulkTones : 1;
+    c64 z[NT];
+    int ntone[3] = {0, 0, 0};
+    ToneConst* tcw = nullptr;
+    if constexpr (FIELD == FIELD_TONES) {
+        __shared__ ToneConst tone_const[kEvolveThreadsMax / 32][NT];
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        tcw = tone_const[warp];
+        __syncwarp();
+        if (lane < NT) {
+            const int c = lane / kBulkTones, k = lane % kBulkTones;
+            ToneConst q = ToneConst{1.0, 0.0, 1.0, 0.0, 0.0};
+            if (k < f.tone_count[c]) {
+                const double* tone = f.tones + 3 * (f.tone_start[c] + k);
+                const double w = __ldg(tone);
+                sincos(w * dt, &q.rot_im, &q.rot_re);
+                sincos(w * a_lo, &q.off_im, &q.off_re);
+                q.amp = f.gain[c] * __ldg(tone + 1);
+            }
+            tcw[lane] = q;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            ntone[c] = f.tone_count[c] < kBulkTones ? f.tone_count[c] : kBulkTones;
+#pragma unroll
+            for (int k = 0; k < kBulkTones; k++) {
+                const int idx = c * kBulkTones + k;
+                z[idx] = c64{0.0, 0.0};
+                if (k < ntone[c] && K > 0) {
+                    const double* tone = f.tones + 3 * (f.tone_start[c] + k);
+                    sincos(fma(__ldg(tone), t_fine, __ldg(tone + 2)), &z[idx].im, &z[idx].re);
+                }
+            }
+        }
+    }
+
+    // Interval product: an FP64 SU(2) element while every step is one (spin half always; spin one
+    // while the quadratic shift is zero), else a full FP64 3x3 matrix.
+    Su2d su2 = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
+    Mat<D> u;
+    set_identity(u);
+    bool in_su2 = true;
+
+    for (int j = j0; j < j1; j++) {
+        // ---- field samples at the two Gauss points (FP64)
+        if constexpr (FIELD == FIELD_TONES) {
+#pragma unroll
+            for (int c = 0; c < L; c++) {
+                double acc_a = f.bias[c], acc_b = f.bias[c];
+                if (c < 3) {
+#pragma unroll
+                    for (int k = 0; k < kBulkTones; k++) {
+                        const int idx = c * kBulkTones + k;
+                        if (k < ntone[c]) {
+                            const ToneConst q = tcw[idx];
+                            const c64 zn = c64{fma(z[idx].re, q.rot_re, -z[idx].im * q.rot_im),
+                                               fma(z[idx].re, q.rot_im, z[idx].im * q.rot_re)};
+                            // sin at t + a_lo = Im(z exp(i w a_lo)); at t + a_hi = Im(z_next exp(-i w a_lo))
+                            const double sa = fma(z[idx].im, q.off_re, z[idx].re * q.off_im);
+                            const double sb = fma(zn.im, q.off_re, -zn.re * q.off_im);
+                            acc_a = fma(q.amp, sa, acc_a);
+                            acc_b = fma(q.amp, sb, acc_b);
+                            z[idx] = zn;
+                        }
+                    }
+                }
+                // tones past the register budget and the quadratic-shift channel: direct evaluation
+                for (int k = (c < 3 ? ntone[c] : 0); k < f.tone_count[c]; k++) {
+                    const double* tone = f.tones + 3 * (f.tone_start[c] + k);
+                    const double w = __ldg(tone), a = f.gain[c] * __ldg(tone + 1), ph = __ldg(tone + 2);
+                    acc_a = fma(a, sin(fma(w, t_fine + a_lo, ph)), acc_a);
+                    acc_b = fma(a, sin(fma(w, t_fine + a_hi, ph)), acc_b);
+                }
+                s0[c] = acc_a;
+                s1[c] = acc_b;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < L; k++) {
+                s0[k] = 0.0;
+                s1[k] = 0.0;
+            }
+            sample_field<FIELD, L>(f, t_fine + a_lo, s0);
+            sample_field<FIELD, L>(f, t_fine + a_hi, s1);
+        }
+        // ---- rotating frame (FP64): xy times exp(-i P rw tau), z minus P rw
+        if (m.rotating) {
+            const c64 Wn = W * Wrot;
+            const c64 xa = c64{s0[0], s0[1]} * (W * Woff);
+            const c64 xb = c64{s1[0], s1[1]} * (Wn * conj(Woff));
+            s0[0] = xa.re;
+            s0[1] = xa.im;
+            s1[0] = xb.re;
+            s1[1] = xb.im;
+            s0[2] -= (double)P * rw;
+            s1[2] -= (double)P * rw;
+            W = Wn;
+        }
+        // ---- CF4 generators: FP64 combinations, each rounded once to FP32
+        float ga[4], gb[4];
+#pragma unroll
+        for (int k = 0; k < L; k++) {
+            ga[k] = __double2float_rn(fma(c0, s0[k], c1 * s1[k]));
+            gb[k] = __double2float_rn(fma(c1, s0[k], c0 * s1[k]));
+        }
+        bool su2_step = true;
+        if constexpr (D == 3) su2_step = (ga[3] == 0.0f && gb[3] == 0.0f);
+        if (su2_step) {
+            const Su2f e = su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2]));
+            if (in_su2) {
+                su2_apply(su2, e);
+            } else if constexpr (D == 3) {
+                u = matmul(su2_to_spin_one(c64{1.0 + (double)e.am1.re, (double)e.am1.im},
+                                           c64{(double)e.beta.re, (double)e.beta.im}), u);
+            }
+        } else if constexpr (D == 3) {
+            if (in_su2) {
+                u = su2_to_spin_one(c64{1.0 + su2.am1.re, su2.am1.im}, su2.beta);
+                in_su2 = false;
+            }
+            const Mat32<3> ea = spin_one_exp_m1(ga[0], ga[1], ga[2], ga[3]);
+            const Mat32<3> eb = spin_one_exp_m1(gb[0], gb[1], gb[2], gb[3]);
+            apply_m1<3>(u, mul_m1_f<3>(eb, ea));
+        }
+        t_fine += dt;
+    }
+    if (in_su2) {
+        const c64 alpha = c64{1.0 + su2.am1.re, su2.am1.im};
+        if constexpr (D == 3) {
+            u = su2_to_spin_one(alpha, su2.beta);
+        } else {
+            u.a[0][0] = alpha;
+            u.a[1][0] = su2.beta;
+            u.a[0][1] = c64{-su2.beta.re, su2.beta.im};
+            u.a[1][1] = conj(alpha);
+        }
+    }
+
+    for (int s = 1; s < lanes; s <<= 1) {
+        const Mat<D> later = shfl_down_mat(u, s);
+        if ((lane_in_group & (2 * s - 1)) == 0) u = matmul(later, u);
+    }
+    if (!active || lane_in_group != 0) return;
+    if (m.rotating) {  // leave the rotating frame, I:839-852
+        c64 wo;
+        sincos(rw * dt_out, &wo.im, &wo.re);
+        const c64 woc = conj(wo);
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            u.a[0][k] = u.a[0][k] * woc;
+            u.a[D - 1][k] = u.a[D - 1][k] * wo;
+        }
+    }
+    time_out[index] = t_c;
+    double2* dst = reinterpret_cast<double2*>(u_out) + index * (D * D);
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int k = 0; k < D; k++) dst[i * D + k] = make_double2(u.a[i][k].re, u.a[i][k].im);
 }
 
 }  // namespace spinsim

@@ -158,6 +158,66 @@ class ToneField(BuiltinField):
         return out
 
 
+def pack_fields(fields, device):
+    """Device structs for a list of built-in fields with one host-to-device copy.
+
+    All tone arrays, table arrays and table descriptors go into one float64 buffer; returns
+    (list of ctypes Field, [device buffer], host bytes copied)."""
+    import ctypes
+    import torch
+    chunks = []
+    n = 0
+
+    def put(arr):
+        nonlocal n
+        arr = np.ascontiguousarray(arr, np.float64).reshape(-1)
+        off = n
+        chunks.append(arr)
+        n += arr.size
+        pad = (-n) % 4  # keep every chunk 32-byte aligned
+        if pad:
+            chunks.append(np.zeros(pad))
+            n += pad
+        return off
+
+    plan = []
+    for f in fields:
+        if isinstance(f, ToneField):
+            flat, start, count = f.packed()
+            plan.append(("tones", f, put(flat), start, count))
+        elif isinstance(f, TabulatedField):
+            offs = {idx: (put(t), put(a), t.size, o, zb) for idx, (t, a, o, zb) in f.tables.items()}
+            tab_off = put(np.zeros(8 * ctypes.sizeof(_lib.Table) // 8))
+            plan.append(("table", f, tab_off, offs, None))
+        else:
+            raise TypeError("not a built-in field")
+    host = np.concatenate(chunks) if chunks else np.zeros(4)
+    dev = torch.empty(host.size, dtype=torch.float64, device=device)
+    base = dev.data_ptr()
+    out = []
+    for kind, f, off, a, b in plan:
+        st = _lib.Field()
+        if kind == "tones":
+            st.tones = base + 8 * off
+            for c in range(8):
+                st.tone_start[c] = int(a[c])
+                st.tone_count[c] = int(b[c])
+                st.bias[c] = f.bias[c]
+                st.gain[c] = 1.0
+        else:
+            tabs = (_lib.Table * 8)()
+            for idx, (to, ao, size, o, zb) in a.items():
+                tabs[idx] = _lib.Table(base + 8 * to, base + 8 * ao, size, o, int(zb))
+            host[off:off + 8 * ctypes.sizeof(_lib.Table) // 8] = np.frombuffer(bytes(tabs), np.float64)
+            st.tables = base + 8 * off
+            for c in range(8):
+                st.bias[c] = f.bias[c]
+                st.gain[c] = f.gain[c]
+        out.append(st)
+    dev.copy_(torch.from_numpy(host))
+    return out, [dev], host.nbytes
+
+
 # ---------------------------------------------------------------------------- sampler factory
 def _sampler_body(time, amplitude, order, zero_boundary):
     """Python source-level sampler (compiled by numba for CUDA or CPU).  Restates the reference's

@@ -87,3 +87,77 @@ def test_graph_replay_reproduces(cuda):
     b.replay()
     torch.cuda.synchronize()
     assert torch.equal(first, b.state)
+
+
+def final_state_errors(a, b):
+    return np.array([np.abs(x - y).max() if x.size else 0.0 for x, y in zip(a.final_states(), b.final_states())])
+
+
+def test_fp32_bulk_tones_error_vs_fp64(cuda):
+    """The batched FP32-bulk form against the plain FP64 form: final-state error <= 1e-6 (uneven
+    spin-half / spin-one tone batch, durations up to 2 ms)."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    insts = make_instances(64, seed=11, max_duration=2e-3)
+    plans = {}
+    bulk = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+    plain = B.Batch(insts, precision=ss.Precision.FP64, plan_cache=plans)
+    bulk.run()
+    plain.run()
+    errs = final_state_errors(bulk, plain)
+    assert errs.max() < 1e-6, errs.max()
+    du = (bulk.u - plain.u).abs().max().item()
+    assert du < 1e-8, du
+
+
+def test_fp32_bulk_quadratic_shift_and_lie_trotter_half(cuda):
+    """Spin one with a quadratic shift (Taylor-series exponential) and spin half with the
+    Lie-Trotter exponentiator selected, against FP64."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    rng = np.random.default_rng(21)
+    insts = []
+    for k in range(12):
+        spin = ss.SpinQuantumNumber.ONE
+        p = F.tone_parameters(np.random.default_rng(500 + k))
+        fld = tone_field(p)
+        fld.bias[3] = ss.fields.TAU * rng.uniform(-20e3, 20e3)
+        fld.tones[3] = np.array([(ss.fields.TAU * 3e5, ss.fields.TAU * 5e3, 0.3)])
+        insts.append(B.Instance(spin, 0.0, 500e-6, 10e-9, 1e-6, spin.plus_x, field=fld))
+    plans = {}
+    bulk = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+    plain = B.Batch(insts, precision=ss.Precision.FP64, plan_cache=plans)
+    bulk.run()
+    plain.run()
+    assert final_state_errors(bulk, plain).max() < 1e-6
+    half = make_instances(24, seed=4, max_duration=1e-3)
+    half = [i for i in half if i.spin.dimension == 2]
+    bulk = B.Batch(half, precision=ss.Precision.FP32_BULK, exponentiation_half=ss.ExponentiationMethod.LIE_TROTTER)
+    plain = B.Batch(half, precision=ss.Precision.FP64, exponentiation_half=ss.ExponentiationMethod.LIE_TROTTER)
+    bulk.run()
+    plain.run()
+    assert final_state_errors(bulk, plain).max() < 1e-6
+
+
+def test_fp32_bulk_gaussian_ensemble_members(cuda):
+    """Spin-half Gaussian-pulse ensemble (user field) in FP32-bulk, per-member error against FP64."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    members = np.random.default_rng(seed=2).normal(0.0, 500.0, 256)
+    insts = [B.Instance(ss.SpinQuantumNumber.HALF, 0.0, 1e-3, 20e-9, 1e-6, ss.SpinQuantumNumber.HALF.plus_z,
+                        sweep_parameters=[m]) for m in members]
+    bulk = B.Batch(insts, get_field=F.gaussian_ensemble, precision=ss.Precision.FP32_BULK)
+    plain = B.Batch(insts, get_field=F.gaussian_ensemble, precision=ss.Precision.FP64)
+    bulk.run()
+    plain.run()
+    errs = final_state_errors(bulk, plain)
+    assert errs.max() < 1e-6, errs.max()
+
+
+def test_fp32_bulk_simulator_single_instance(cuda):
+    import spinsim_b200 as ss
+    sim32 = ss.Simulator(F.detuned_rabi, ss.SpinQuantumNumber.ONE, precision=ss.Precision.FP32_BULK)
+    sim64 = ss.Simulator(F.detuned_rabi, ss.SpinQuantumNumber.ONE)
+    a = sim32.evaluate(0, 1e-3, 10e-9, 100e-9, ss.SpinQuantumNumber.ONE.plus_z, [250.0])
+    b = sim64.evaluate(0, 1e-3, 10e-9, 100e-9, ss.SpinQuantumNumber.ONE.plus_z, [250.0])
+    assert np.abs(a.state - b.state).max() < 1e-6

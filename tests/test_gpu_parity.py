@@ -46,7 +46,7 @@ def simulator(c, field=None, **kw):
     if key not in _sims:
         if field is None:
             field = user_table_field(c) if c["field"] == "table" else F.FIELDS[c["field"]]
-        expo = ss.ExponentiationMethod(c["exponentiation"]) if c["exponentiation"] else None
+        expo = {m.value: m for m in ss.ExponentiationMethod}[c["exponentiation"]] if c["exponentiation"] else None
         _sims[key] = ss.Simulator(field, spin_of(c["spin"]), exponentiation_method=expo,
                                   use_rotating_frame=c["rotating"],
                                   integration_method=ss.IntegrationMethod(c["integration"]),
