@@ -21,7 +21,6 @@ batch of the same shape from its own seeds; no collective on the data path).
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -94,58 +93,53 @@ def algorithmic_flops(specs, form):
 
 # ------------------------------------------------------------------------------------ helpers
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every 10 ms during the timed region."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                        r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for name, bit in self.REASONS.items():
+                            if r & bit:
+                                self.reasons.add(name)
+                    except Exception:
+                        pass
+                    self._stop.wait(0.01)
+
+            self.thread = threading.Thread(target=run, daemon=True)
             self.thread.start()
-        except (OSError, ValueError):
-            self.proc = None
+        except Exception:
+            self.thread = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self._stop.set()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[3:7]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
 
 
 def peaks_from_file():
@@ -226,8 +220,11 @@ def bench_ours(args, world, rank):
     insts = instances(ss, specs)
     total_steps = sum(int(d / 1e-6) * 100 for _, d, _ in specs)
     plans = {}
-    bulk = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
-    plain = Batch(insts, precision=ss.Precision.FP64, plan_cache=plans)
+    from spinsim_b200.autotune import tune
+    cfg_bulk, tune_bulk = tune(insts, use_cache=False, precision=ss.Precision.FP32_BULK)
+    cfg_plain, tune_plain = tune(insts, use_cache=False, precision=ss.Precision.FP64)
+    bulk = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans, **cfg_bulk)
+    plain = Batch(insts, precision=ss.Precision.FP64, plan_cache=plans, **cfg_plain)
     assert bulk.total_steps == total_steps
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
 
@@ -278,7 +275,7 @@ def bench_ours(args, world, rank):
     for it in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        b = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+        b = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans, **cfg_bulk)
         b.run()
         outs = [b.time, b.u, b.state, b.spin]
         if pinned is None:
@@ -320,8 +317,11 @@ def bench_ours(args, world, rank):
                                "durations log-uniform 10us-10ms, dt_int 10ns, dt_out 1us, 8 tones per axis, "
                                "Magnus CF4, rotating frame, one persistent launch (CUDA graph)",
                    "instances_per_gpu": len(specs), "integration_steps_per_gpu": total_steps,
-                   "l2": "256 MB buffer written between timed steps", "lanes": info["lanes"],
-                   "threads_per_block": info["threads_per_block"], "registers": info["registers_per_thread"]},
+                   "l2": "256 MB buffer written between timed steps",
+                   "autotuned": {"fp32_bulk": cfg_bulk, "fp64": cfg_plain},
+                   "threads_per_block": info["threads_per_block"], "registers": info["registers_per_thread"],
+                   "tuning_ms": {"fp32_bulk": {k: 1e3 * v for k, v in tune_bulk.items()},
+                                 "fp64": {k: 1e3 * v for k, v in tune_plain.items()}}},
         "latency_ms": {"p50": 1e3 * float(np.percentile(t_bulk, 50)), "p99": 1e3 * float(np.percentile(t_bulk, 99))},
         "plain_fp64": {"value": world * total_steps * args.steps / t_plain_total, "unit": "steps/s",
                        "ms_per_step": 1e3 * t_plain_total / args.steps,
@@ -410,7 +410,7 @@ def bench_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -58,8 +58,9 @@ typedef struct {
     int32_t number_of_squares; /* number_of_squares (north_star: trotter_cutoff), >= 0 */
     int32_t field_kind;        /* SPINSIM_FIELD_* */
     int32_t precision;         /* SPINSIM_PRECISION_* */
-    int32_t threads_per_block; /* 0 = library default; else a multiple of 32, <= 1024 */
-    int32_t max_registers;     /* 0 = default; user-field plans pass it to the JIT linker */
+    int32_t threads_per_block; /* 0 = library default (128); else a multiple of 32, <= 128 */
+    int32_t max_registers;     /* 0 = no cap; <= 128 selects the 128-register build (built-in fields)
+                                  or is passed to the JIT linker (user fields) */
     int32_t lanes;             /* lanes per output interval: 0 = auto, else 1, 2, 4, 8, 16 or 32 */
     int32_t reserved;
 } spinsim_plan_desc;

@@ -268,7 +268,8 @@ class Simulator:
         desc.number_of_squares = nsq
         desc.field_kind = field_kind
         desc.precision = self.precision.value
-        desc.threads_per_block = tpb if tpb in (32, 64, 96, 128, 160, 192, 224, 256) else 0
+        # threads_per_block (a tuning knob of the reference, I:375) is honoured up to the kernel's 128
+        desc.threads_per_block = max(32, min(128, tpb // 32 * 32)) if tpb else 0
         desc.max_registers = int(opts["max_registers"] or 0)
         desc.lanes = int(lanes)
         lib = _lib.load()

@@ -42,13 +42,14 @@ class Batch:
     Parameters mirror Simulator: ``get_field`` (a user function shared by all instances, or None for
     per-instance built-in fields), ``integration_method``, ``exponentiation_half`` /
     ``exponentiation_one`` (defaults: analytic for spin half, Lie-Trotter for spin one, I:529-533),
-    ``use_rotating_frame``, ``number_of_squares``, ``precision``, ``lanes``, ``threads_per_block``.
+    ``use_rotating_frame``, ``number_of_squares``, ``precision``, ``lanes``, ``threads_per_block``,
+    ``max_registers`` (the last three are picked by ``spinsim_b200.autotune.tune``).
     """
 
     def __init__(self, instances, get_field=None, integration_method=IntegrationMethod.MAGNUS_CF4,
                  exponentiation_half=ExponentiationMethod.ANALYTIC, exponentiation_one=ExponentiationMethod.LIE_TROTTER,
                  use_rotating_frame=True, number_of_squares=24, precision=Precision.FP64, lanes=0,
-                 threads_per_block=0, plan_cache=None):
+                 threads_per_block=0, max_registers=0, plan_cache=None):
         import torch
         self.instances = list(instances)
         if not self.instances:
@@ -80,6 +81,9 @@ class Batch:
         desc.precision = Precision(precision).value
         desc.threads_per_block = int(threads_per_block)
         desc.lanes = int(lanes)
+        desc.max_registers = int(max_registers)
+        self.config = {"lanes": int(lanes), "threads_per_block": int(threads_per_block),
+                       "max_registers": int(max_registers)}
         self.lib = lib = _lib.load()
         key = bytes(desc) + (ltoir or b"")
         if plan_cache is not None and key in plan_cache:

@@ -29,7 +29,7 @@ enum Precision : int { PREC_FP64 = 0, PREC_FP32_BULK = 1 };
 
 constexpr int kMaxChannels = 8;  // x, y, z, q, u1, u2, v1, v2 (reference docs I:381-389)
 constexpr int kEvolveThreadsDefault = 128;  // time-evolution CTA size unless the plan asks otherwise
-constexpr int kEvolveThreadsMax = 256;      // __launch_bounds__ of the time-evolution kernels
+constexpr int kEvolveThreadsMax = 128;      // __launch_bounds__ of the time-evolution kernels
 
 // ------------------------------------------------------------------ field descriptors
 // One interpolation table (the reference's generate_interpolation_sampler, I:1941-2147).

@@ -220,10 +220,11 @@ SS_D void su2_apply(Su2d& p, const Su2f& e) {
 constexpr int kBulkTones = 8;  // tones per channel (x, y, z) carried as FP64 phasors in registers
 
 // Per-instance tone constants, shared by the warp (all its lanes work on one instance).
+// A tone is carried as u = A exp(i (w (t + a_lo) + phi)), t the step start: the sample at the first
+// Gauss point is Im(u); at the second, Im(u exp(i w (a_hi - a_lo))); the next step's u is u exp(i w dt).
 struct ToneConst {
     double rot_re, rot_im;  // exp(i w dt)
-    double off_re, off_im;  // exp(i w a_lo)
-    double amp;             // gain * A
+    double gap_re, gap_im;  // exp(i w (a_hi - a_lo))
 };
 
 template <int D, int INTEG, int EXPO, int FIELD>
@@ -235,7 +236,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lanes = m.lanes;
     const double dt = inst.dt_int, dt_out = inst.dt_out;
-    const double t_c = inst.t0 + dt_out * (double)index;
+    const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)index));  // I:818, unfused
     double s0[8], s1[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -279,13 +280,11 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         __syncwarp();
         if (lane < NT) {
             const int c = lane / kBulkTones, k = lane % kBulkTones;
-            ToneConst q = ToneConst{1.0, 0.0, 1.0, 0.0, 0.0};
+            ToneConst q = ToneConst{1.0, 0.0, 1.0, 0.0};
             if (k < f.tone_count[c]) {
-                const double* tone = f.tones + 3 * (f.tone_start[c] + k);
-                const double w = __ldg(tone);
+                const double w = __ldg(f.tones + 3 * (f.tone_start[c] + k));
                 sincos(w * dt, &q.rot_im, &q.rot_re);
-                sincos(w * a_lo, &q.off_im, &q.off_re);
-                q.amp = f.gain[c] * __ldg(tone + 1);
+                sincos(w * (a_hi - a_lo), &q.gap_im, &q.gap_re);
             }
             tcw[lane] = q;
         }
@@ -299,41 +298,43 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
                 z[idx] = c64{0.0, 0.0};
                 if (k < ntone[c] && K > 0) {
                     const double* tone = f.tones + 3 * (f.tone_start[c] + k);
-                    sincos(fma(__ldg(tone), t_fine, __ldg(tone + 2)), &z[idx].im, &z[idx].re);
+                    const double amp = f.gain[c] * __ldg(tone + 1);
+                    double sn, cs;
+                    sincos(fma(__ldg(tone), t_fine + a_lo, __ldg(tone + 2)), &sn, &cs);
+                    z[idx] = c64{amp * cs, amp * sn};
                 }
             }
         }
     }
 
-    // Interval product: an FP64 SU(2) element while every step is one (spin half always; spin one
-    // while the quadratic shift is zero), else a full FP64 3x3 matrix.
-    Su2d su2 = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
-    Mat<D> u;
-    set_identity(u);
-    bool in_su2 = true;
-
-    for (int j = j0; j < j1; j++) {
-        // ---- field samples at the two Gauss points (FP64)
+    // One step's field samples (FP64) -> frame transform -> CF4 generators rounded to FP32.
+    // Advances the tone and frame recurrences.
+    auto step_generators = [&](float* ga, float* gb) {
         if constexpr (FIELD == FIELD_TONES) {
 #pragma unroll
             for (int c = 0; c < L; c++) {
                 double acc_a = f.bias[c], acc_b = f.bias[c];
                 if (c < 3) {
+                    // two partial sums per Gauss point keep the dependent add chains short
+                    double pa = 0.0, pb = 0.0;
 #pragma unroll
                     for (int k = 0; k < kBulkTones; k++) {
                         const int idx = c * kBulkTones + k;
                         if (k < ntone[c]) {
                             const ToneConst q = tcw[idx];
-                            const c64 zn = c64{fma(z[idx].re, q.rot_re, -z[idx].im * q.rot_im),
-                                               fma(z[idx].re, q.rot_im, z[idx].im * q.rot_re)};
-                            // sin at t + a_lo = Im(z exp(i w a_lo)); at t + a_hi = Im(z_next exp(-i w a_lo))
-                            const double sa = fma(z[idx].im, q.off_re, z[idx].re * q.off_im);
-                            const double sb = fma(zn.im, q.off_re, -zn.re * q.off_im);
-                            acc_a = fma(q.amp, sa, acc_a);
-                            acc_b = fma(q.amp, sb, acc_b);
-                            z[idx] = zn;
+                            const c64 v = z[idx];
+                            if (k & 1) {
+                                pa += v.im;
+                                pb = fma(v.re, q.gap_im, fma(v.im, q.gap_re, pb));
+                            } else {
+                                acc_a += v.im;
+                                acc_b = fma(v.re, q.gap_im, fma(v.im, q.gap_re, acc_b));
+                            }
+                            z[idx] = c64{fma(v.re, q.rot_re, -v.im * q.rot_im), fma(v.re, q.rot_im, v.im * q.rot_re)};
                         }
                     }
+                    acc_a += pa;
+                    acc_b += pb;
                 }
                 // tones past the register budget and the quadratic-shift channel: direct evaluation
                 for (int k = (c < 3 ? ntone[c] : 0); k < f.tone_count[c]; k++) {
@@ -354,8 +355,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             sample_field<FIELD, L>(f, t_fine + a_lo, s0);
             sample_field<FIELD, L>(f, t_fine + a_hi, s1);
         }
-        // ---- rotating frame (FP64): xy times exp(-i P rw tau), z minus P rw
-        if (m.rotating) {
+        if (m.rotating) {  // xy times exp(-i P rw tau), z minus P rw
             const c64 Wn = W * Wrot;
             const c64 xa = c64{s0[0], s0[1]} * (W * Woff);
             const c64 xb = c64{s1[0], s1[1]} * (Wn * conj(Woff));
@@ -367,35 +367,43 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             s1[2] -= (double)P * rw;
             W = Wn;
         }
-        // ---- CF4 generators: FP64 combinations, each rounded once to FP32
-        float ga[4], gb[4];
 #pragma unroll
         for (int k = 0; k < L; k++) {
             ga[k] = __double2float_rn(fma(c0, s0[k], c1 * s1[k]));
             gb[k] = __double2float_rn(fma(c1, s0[k], c0 * s1[k]));
         }
-        bool su2_step = true;
-        if constexpr (D == 3) su2_step = (ga[3] == 0.0f && gb[3] == 0.0f);
-        if (su2_step) {
-            const Su2f e = su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2]));
-            if (in_su2) {
-                su2_apply(su2, e);
-            } else if constexpr (D == 3) {
-                u = matmul(su2_to_spin_one(c64{1.0 + (double)e.am1.re, (double)e.am1.im},
-                                           c64{(double)e.beta.re, (double)e.beta.im}), u);
+    };
+
+    // Phase 1: every step an SU(2) element (spin half always; spin one while the quadratic shift
+    // is zero); the interval product is an FP64 SU(2) element.
+    Su2d su2 = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
+    float ga[4] = {0.0f, 0.0f, 0.0f, 0.0f}, gb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    int j = j0;
+    bool pending = false;
+    // Software-pipelined: the next step's field samples (independent FP64 work) are issued next
+    // to this step's exponential and product (a dependent chain), so they overlap.
+    if (j < j1) step_generators(ga, gb);
+    for (; j < j1; j++) {
+        if constexpr (D == 3) {
+            if (ga[3] != 0.0f || gb[3] != 0.0f) {
+                pending = true;
+                break;
             }
-        } else if constexpr (D == 3) {
-            if (in_su2) {
-                u = su2_to_spin_one(c64{1.0 + su2.am1.re, su2.am1.im}, su2.beta);
-                in_su2 = false;
-            }
-            const Mat32<3> ea = spin_one_exp_m1(ga[0], ga[1], ga[2], ga[3]);
-            const Mat32<3> eb = spin_one_exp_m1(gb[0], gb[1], gb[2], gb[3]);
-            apply_m1<3>(u, mul_m1_f<3>(eb, ea));
         }
+        float na[4] = {0.0f, 0.0f, 0.0f, 0.0f}, nb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        const double t_step = t_fine;
         t_fine += dt;
+        if (j + 1 < j1) step_generators(na, nb);
+        su2_apply(su2, su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2])));
+        (void)t_step;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            ga[k] = na[k];
+            gb[k] = nb[k];
+        }
     }
-    if (in_su2) {
+    Mat<D> u;
+    {
         const c64 alpha = c64{1.0 + su2.am1.re, su2.am1.im};
         if constexpr (D == 3) {
             u = su2_to_spin_one(alpha, su2.beta);
@@ -404,6 +412,19 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             u.a[1][0] = su2.beta;
             u.a[0][1] = c64{-su2.beta.re, su2.beta.im};
             u.a[1][1] = conj(alpha);
+        }
+    }
+    // Phase 2 (spin one with a quadratic shift): full 3x3 exponentials and an FP64 3x3 product.
+    if constexpr (D == 3) {
+        if (pending) {
+            for (; j < j1; j++) {
+                if (!pending) step_generators(ga, gb);
+                pending = false;
+                const Mat32<3> ea = spin_one_exp_m1(ga[0], ga[1], ga[2], ga[3]);
+                const Mat32<3> eb = spin_one_exp_m1(gb[0], gb[1], gb[2], gb[3]);
+                apply_m1<3>(u, mul_m1_f<3>(eb, ea));
+                t_fine += dt;
+            }
         }
     }
 

@@ -63,8 +63,10 @@ SS_D void evolve_body(const EvolveArgs& a) {
     }
 }
 
-template <int DIMS, int INTEG, int EXPO_H, int EXPO_O, int FIELD, int PREC>
-__global__ void __launch_bounds__(kEvolveThreadsMax) evolve_kernel(EvolveArgs a) {
+// MINB = minimum resident CTAs per SM that the register allocation must allow (128-thread CTAs):
+// 2 leaves the full register file to one thread (255), 3 caps at 168, 4 at 128 registers.
+template <int DIMS, int INTEG, int EXPO_H, int EXPO_O, int FIELD, int PREC, int MINB>
+__global__ void __launch_bounds__(kEvolveThreadsMax, MINB) evolve_kernel(EvolveArgs a) {
     evolve_body<DIMS, INTEG, EXPO_H, EXPO_O, FIELD, PREC>(a);
 }
 
