@@ -15,7 +15,7 @@ import numpy as np
 _lock = threading.Lock()
 DEFAULT_CANDIDATES = [
     {"lanes": lanes, "threads_per_block": tpb, "max_registers": regs}
-    for regs in (0, 128) for lanes in (1, 2) for tpb in (64, 128)
+    for regs in (0, 168, 128) for lanes in (1, 2) for tpb in (64, 128)
 ]
 
 

@@ -101,6 +101,16 @@ struct EvolveArgs {
     double* u;               // complex [sum N * d * d]; instance i starts at u_offset doubles
 };
 
+// ------------------------------------------------------------------ FP32-bulk tone synthesis
+// Shared memory of the FP32-bulk tone kernels (see evolve32.cuh), per warp.
+constexpr int kBulkTones = 8;               // tones per channel (x, y, z) synthesised per warp
+constexpr int kToneSlots = 3 * kBulkTones;  // slot = channel * kBulkTones + tone
+struct ToneShared {
+    double l[kToneSlots][32][2];  // [slot][lane] (re, im) of the lane's L = A exp(i (w t_c + phi))
+    double uv[2][kToneSlots][4];  // [buffer][slot] U.re, U.im, V.re, V.im of the current step
+};
+constexpr int kToneSharedBytes = kToneSlots * 32 * 2 * 8 + 2 * kToneSlots * 4 * 8;
+
 // ------------------------------------------------------------------ complex helpers (FP64)
 struct c64 {
     double re, im;

@@ -216,16 +216,16 @@ SS_D void su2_apply(Su2d& p, const Su2f& e) {
     p.beta = nb;
 }
 
-// ---------------------------------------------------------------------------------- tone recurrences
-constexpr int kBulkTones = 8;  // tones per channel (x, y, z) carried as FP64 phasors in registers
-
-// Per-instance tone constants, shared by the warp (all its lanes work on one instance).
-// A tone is carried as u = A exp(i (w (t + a_lo) + phi)), t the step start: the sample at the first
-// Gauss point is Im(u); at the second, Im(u exp(i w (a_hi - a_lo))); the next step's u is u exp(i w dt).
-struct ToneConst {
-    double rot_re, rot_im;  // exp(i w dt)
-    double gap_re, gap_im;  // exp(i w (a_hi - a_lo))
-};
+// ---------------------------------------------------------------------------------- tone synthesis
+// Warp-cooperative evaluation of tone fields (FIELD_TONES).  The 32 lanes of a warp work on
+// consecutive output intervals of one instance and step through their fine steps in lockstep, so
+// the sample times differ between lanes only by the interval start t_c.  Writing
+//     A sin(w (t_c + tau) + phi) = Im( L(t_c) U(tau) ),  L = A exp(i (w t_c + phi)),  U = exp(i w tau),
+// each lane keeps its L for the interval in shared memory (read-only), while U(tau) for the current
+// step is the same for the whole warp: lane k advances tone k's U by an FP64 recurrence
+// (U <- U exp(i w dt)) and publishes it, with V = U exp(i w (a_hi - a_lo)) for the second Gauss
+// point, through a double-buffered shared slot.  Per lane and tone a sample then costs two FMAs.
+static_assert(sizeof(ToneShared) == kToneSharedBytes, "tone shared layout");
 
 template <int D, int INTEG, int EXPO, int FIELD>
 SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDesc& f, int64_t index, bool active,
@@ -234,7 +234,8 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     static_assert(EXPO != EXPO_LIE_TROTTER_8, "the FP32-bulk form has no eight-generator exponential");
     constexpr int L = (D == 2) ? 3 : 4;
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
-    const int lanes = m.lanes;
+    constexpr bool TONES = (FIELD == FIELD_TONES);
+    const int lanes = TONES ? 1 : m.lanes;  // tone synthesis runs the warp's lanes in lockstep
     const double dt = inst.dt_int, dt_out = inst.dt_out;
     const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)index));  // I:818, unfused
     double s0[8], s1[8];
@@ -249,7 +250,9 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         rw = s0[2];
         if (D == 2) rw /= 2;
     }
-    const int K = active ? inst.n_fine : 0;
+    // With tone synthesis every lane of the warp runs the instance's K steps (inactive lanes only
+    // publish tone phasors); otherwise inactive lanes run none.
+    const int K = (active || TONES) ? inst.n_fine : 0;
     const int j0 = (int)(((int64_t)K * lane_in_group) / lanes);
     const int j1 = (int)(((int64_t)K * (lane_in_group + 1)) / lanes);
     double t_fine = t_c;
@@ -268,80 +271,91 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         sincos(-(double)P * rw * a_lo, &Woff.im, &Woff.re);
     }
 
-    // Tone phasors z = exp(i (w t + phi)) at the step start, FP64 (FIELD_TONES only).
-    constexpr int NT = (FIELD == FIELD_TONES) ? 3 * kBulkTones : 1;
-    c64 z[NT];
-    int ntone[3] = {0, 0, 0};
-    ToneConst* tcw = nullptr;
-    if constexpr (FIELD == FIELD_TONES) {
-        __shared__ ToneConst tone_const[kEvolveThreadsMax / 32][NT];
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        tcw = tone_const[warp];
-        __syncwarp();
-        if (lane < NT) {
+    double bias[L];
+#pragma unroll
+    for (int c = 0; c < L; c++) bias[c] = f.bias[c];
+
+    // ---- tone synthesis set-up (FIELD_TONES)
+    ToneShared* ts = nullptr;
+    const int lane = threadIdx.x & 31;
+    c64 u_prod = c64{0.0, 0.0}, u_rot = c64{1.0, 0.0}, u_gap = c64{1.0, 0.0};
+    bool direct_tones = false;  // tones beyond kBulkTones on x, y, z, or any tone on q
+    if constexpr (TONES) {
+        extern __shared__ __align__(16) unsigned char spinsim_dyn_smem[];
+        ts = reinterpret_cast<ToneShared*>(spinsim_dyn_smem) + (threadIdx.x >> 5);
+#pragma unroll
+        for (int c = 0; c < L; c++) direct_tones |= f.tone_count[c] > (c < 3 ? kBulkTones : 0);
+        // this lane's L for every slot
+#pragma unroll 1
+        for (int slot = 0; slot < kToneSlots; slot++) {
+            const int c = slot / kBulkTones, k = slot % kBulkTones;
+            double re = 0.0, im = 0.0;
+            if (active && k < f.tone_count[c]) {
+                const double* tone = f.tones + 3 * (f.tone_start[c] + k);
+                const double amp = f.gain[c] * __ldg(tone + 1);
+                double sn, cs;
+                sincos(fma(__ldg(tone), t_c, __ldg(tone + 2)), &sn, &cs);
+                re = amp * cs;
+                im = amp * sn;
+            }
+            ts->l[slot][lane][0] = re;
+            ts->l[slot][lane][1] = im;
+        }
+        // producer lane `lane` owns slot `lane`: U(a_lo), rotation per step, gap to a_hi
+        if (lane < kToneSlots) {
             const int c = lane / kBulkTones, k = lane % kBulkTones;
-            ToneConst q = ToneConst{1.0, 0.0, 1.0, 0.0};
             if (k < f.tone_count[c]) {
                 const double w = __ldg(f.tones + 3 * (f.tone_start[c] + k));
-                sincos(w * dt, &q.rot_im, &q.rot_re);
-                sincos(w * (a_hi - a_lo), &q.gap_im, &q.gap_re);
-            }
-            tcw[lane] = q;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            ntone[c] = f.tone_count[c] < kBulkTones ? f.tone_count[c] : kBulkTones;
-#pragma unroll
-            for (int k = 0; k < kBulkTones; k++) {
-                const int idx = c * kBulkTones + k;
-                z[idx] = c64{0.0, 0.0};
-                if (k < ntone[c] && K > 0) {
-                    const double* tone = f.tones + 3 * (f.tone_start[c] + k);
-                    const double amp = f.gain[c] * __ldg(tone + 1);
-                    double sn, cs;
-                    sincos(fma(__ldg(tone), t_fine + a_lo, __ldg(tone + 2)), &sn, &cs);
-                    z[idx] = c64{amp * cs, amp * sn};
-                }
+                sincos(w * a_lo, &u_prod.im, &u_prod.re);
+                sincos(w * dt, &u_rot.im, &u_rot.re);
+                sincos(w * (a_hi - a_lo), &u_gap.im, &u_gap.re);
             }
         }
     }
 
     // One step's field samples (FP64) -> frame transform -> CF4 generators rounded to FP32.
-    // Advances the tone and frame recurrences.
-    auto step_generators = [&](float* ga, float* gb) {
-        if constexpr (FIELD == FIELD_TONES) {
+    auto step_generators = [&](int j, float* ga, float* gb) {
+        if constexpr (TONES) {
+            // publish U, V of step j, then read them back for every slot
+            if (lane < kToneSlots) {
+                const c64 v = u_prod * u_gap;
+                double* dst = ts->uv[j & 1][lane];
+                dst[0] = u_prod.re;
+                dst[1] = u_prod.im;
+                dst[2] = v.re;
+                dst[3] = v.im;
+                u_prod = u_prod * u_rot;
+            }
+            __syncwarp();
 #pragma unroll
             for (int c = 0; c < L; c++) {
-                double acc_a = f.bias[c], acc_b = f.bias[c];
+                double acc_a = bias[c], acc_b = bias[c];
                 if (c < 3) {
-                    // two partial sums per Gauss point keep the dependent add chains short
                     double pa = 0.0, pb = 0.0;
 #pragma unroll
                     for (int k = 0; k < kBulkTones; k++) {
-                        const int idx = c * kBulkTones + k;
-                        if (k < ntone[c]) {
-                            const ToneConst q = tcw[idx];
-                            const c64 v = z[idx];
-                            if (k & 1) {
-                                pa += v.im;
-                                pb = fma(v.re, q.gap_im, fma(v.im, q.gap_re, pb));
-                            } else {
-                                acc_a += v.im;
-                                acc_b = fma(v.re, q.gap_im, fma(v.im, q.gap_re, acc_b));
-                            }
-                            z[idx] = c64{fma(v.re, q.rot_re, -v.im * q.rot_im), fma(v.re, q.rot_im, v.im * q.rot_re)};
+                        const int slot = c * kBulkTones + k;
+                        const double2 lv = *reinterpret_cast<const double2*>(ts->l[slot][lane]);
+                        const double2 uu = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][0]);
+                        const double2 vv = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][2]);
+                        if (k & 1) {
+                            pa = fma(lv.x, uu.y, fma(lv.y, uu.x, pa));
+                            pb = fma(lv.x, vv.y, fma(lv.y, vv.x, pb));
+                        } else {
+                            acc_a = fma(lv.x, uu.y, fma(lv.y, uu.x, acc_a));
+                            acc_b = fma(lv.x, vv.y, fma(lv.y, vv.x, acc_b));
                         }
                     }
                     acc_a += pa;
                     acc_b += pb;
                 }
-                // tones past the register budget and the quadratic-shift channel: direct evaluation
-                for (int k = (c < 3 ? ntone[c] : 0); k < f.tone_count[c]; k++) {
-                    const double* tone = f.tones + 3 * (f.tone_start[c] + k);
-                    const double w = __ldg(tone), a = f.gain[c] * __ldg(tone + 1), ph = __ldg(tone + 2);
-                    acc_a = fma(a, sin(fma(w, t_fine + a_lo, ph)), acc_a);
-                    acc_b = fma(a, sin(fma(w, t_fine + a_hi, ph)), acc_b);
+                if (direct_tones) {  // tones past the synthesis slots, and the q channel
+                    for (int k = (c < 3 ? kBulkTones : 0); k < f.tone_count[c]; k++) {
+                        const double* tone = f.tones + 3 * (f.tone_start[c] + k);
+                        const double w = __ldg(tone), a = f.gain[c] * __ldg(tone + 1), ph = __ldg(tone + 2);
+                        acc_a = fma(a, sin(fma(w, t_fine + a_lo, ph)), acc_a);
+                        acc_b = fma(a, sin(fma(w, t_fine + a_hi, ph)), acc_b);
+                    }
                 }
                 s0[c] = acc_a;
                 s1[c] = acc_b;
@@ -375,27 +389,31 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     };
 
     // Phase 1: every step an SU(2) element (spin half always; spin one while the quadratic shift
-    // is zero); the interval product is an FP64 SU(2) element.
+    // is zero); the interval product is an FP64 SU(2) element.  Software-pipelined: the next step's
+    // field samples (independent FP64 work) are issued next to this step's exponentials and product.
     Su2d su2 = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
     float ga[4] = {0.0f, 0.0f, 0.0f, 0.0f}, gb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     int j = j0;
     bool pending = false;
-    // Software-pipelined: the next step's field samples (independent FP64 work) are issued next
-    // to this step's exponential and product (a dependent chain), so they overlap.
-    if (j < j1) step_generators(ga, gb);
+    if (j < j1) step_generators(j, ga, gb);
     for (; j < j1; j++) {
-        if constexpr (D == 3) {
+        if constexpr (D == 3 && !TONES) {
             if (ga[3] != 0.0f || gb[3] != 0.0f) {
                 pending = true;
                 break;
             }
         }
+        if constexpr (D == 3 && TONES) {
+            // the whole warp leaves phase 1 together (tone synthesis is in lockstep)
+            if (__any_sync(0xffffffffu, active && (ga[3] != 0.0f || gb[3] != 0.0f))) {
+                pending = true;
+                break;
+            }
+        }
         float na[4] = {0.0f, 0.0f, 0.0f, 0.0f}, nb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        const double t_step = t_fine;
         t_fine += dt;
-        if (j + 1 < j1) step_generators(na, nb);
+        if (j + 1 < j1) step_generators(j + 1, na, nb);
         su2_apply(su2, su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2])));
-        (void)t_step;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             ga[k] = na[k];
@@ -417,9 +435,10 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     // Phase 2 (spin one with a quadratic shift): full 3x3 exponentials and an FP64 3x3 product.
     if constexpr (D == 3) {
         if (pending) {
+            bool first = true;
             for (; j < j1; j++) {
-                if (!pending) step_generators(ga, gb);
-                pending = false;
+                if (!first) step_generators(j, ga, gb);
+                first = false;
                 const Mat32<3> ea = spin_one_exp_m1(ga[0], ga[1], ga[2], ga[3]);
                 const Mat32<3> eb = spin_one_exp_m1(gb[0], gb[1], gb[2], gb[3]);
                 apply_m1<3>(u, mul_m1_f<3>(eb, ea));
@@ -427,6 +446,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             }
         }
     }
+    if constexpr (TONES) __syncwarp();  // the shared slots are reused by the warp's next tile
 
     for (int s = 1; s < lanes; s <<= 1) {
         const Mat<D> later = shfl_down_mat(u, s);
