@@ -407,6 +407,32 @@ def bench_reference(args, world, rank):
     }
 
 
+def bench_serving(args):
+    """Serving workload: Poisson arrivals of evaluate() requests (70% spin half / 30% spin one,
+    durations log-uniform 10 us - 100 ms, dt_int from {10, 20, 50, 100} ns, dt_out 1 us, pulse-train
+    tables), continuous batching under an HBM budget; p50/p99 latency and throughput per rate."""
+    import torch
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Server, latency_summary, synthetic_requests
+    rates = [float(r) for r in args.rates.split(",")]
+    out = {"metric": "serving p50/p99 latency and steps/s", "workload": "serving", "requests_per_rate": args.requests,
+           "precision": "fp32_bulk", "hbm_budget_gb": args.hbm_budget_gb, "rates": {}}
+    warm = synthetic_requests(64, 1e5, seed=99, max_duration=1e-3)
+    Server(precision=ss.Precision.FP32_BULK).run(warm)
+    for rate in rates:
+        reqs = synthetic_requests(args.requests, rate, seed=4)
+        srv = Server(precision=ss.Precision.FP32_BULK, hbm_budget=int(args.hbm_budget_gb * (1 << 30)),
+                     streams=args.streams, max_batch=args.max_batch)
+        torch.cuda.synchronize()
+        done = srv.run(reqs)
+        torch.cuda.synchronize()
+        summ = latency_summary(done)
+        summ.update({"launches": srv.stats["launches"], "budget_waits": srv.stats["budget_waits"]})
+        out["rates"][str(int(rate))] = summ
+        print(json.dumps({"rate": rate, **summ}), file=sys.stderr, flush=True)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -414,6 +440,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="batch", choices=["batch", "serving"])
+    ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
+    ap.add_argument("--requests", type=int, default=20000)
+    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--max-batch", type=int, default=2048)
+    ap.add_argument("--hbm-budget-gb", type=float, default=16.0)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -425,6 +457,10 @@ def main():
         print(json.dumps({"metric": METRIC, "unavailable": "no CUDA device"}))
         return
     torch.cuda.set_device(local)
+    if args.workload == "serving":
+        if rank == 0:
+            print(json.dumps(bench_serving(args)), flush=True)
+        return
     out, specs = bench_ours(args, world, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O

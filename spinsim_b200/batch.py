@@ -43,13 +43,14 @@ class Batch:
     per-instance built-in fields), ``integration_method``, ``exponentiation_half`` /
     ``exponentiation_one`` (defaults: analytic for spin half, Lie-Trotter for spin one, I:529-533),
     ``use_rotating_frame``, ``number_of_squares``, ``precision``, ``lanes``, ``threads_per_block``,
-    ``max_registers`` (the last three are picked by ``spinsim_b200.autotune.tune``).
+    ``max_registers`` (the last three are picked by ``spinsim_b200.autotune.tune``), ``force_mixed``
+    (use the mixed-spin kernel even for a single-spin batch).
     """
 
     def __init__(self, instances, get_field=None, integration_method=IntegrationMethod.MAGNUS_CF4,
                  exponentiation_half=ExponentiationMethod.ANALYTIC, exponentiation_one=ExponentiationMethod.LIE_TROTTER,
                  use_rotating_frame=True, number_of_squares=24, precision=Precision.FP64, lanes=0,
-                 threads_per_block=0, max_registers=0, plan_cache=None):
+                 threads_per_block=0, max_registers=0, plan_cache=None, force_mixed=False):
         import torch
         self.instances = list(instances)
         if not self.instances:
@@ -57,7 +58,8 @@ class Batch:
         dev = _cuda_device()
         self.device = dev
         dims = sorted({i.spin.dimension for i in self.instances})
-        spin_dim = dims[0] if len(dims) == 1 else 0
+        # force_mixed: always the mixed-spin kernel, so results do not depend on the batch's spin mix
+        spin_dim = dims[0] if (len(dims) == 1 and not force_mixed) else 0
         if exponentiation_one == ExponentiationMethod.ANALYTIC:
             exponentiation_one = ExponentiationMethod.LIE_TROTTER
         if get_field is None:

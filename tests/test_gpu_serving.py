@@ -1,0 +1,68 @@
+"""Continuous-batching server: correctness against the oracle, identity of a result alone and in
+the mix, and HBM-budget admission."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_of(req):
+    f = req.field
+    tabs = [(f.tables[0][0], f.tables[0][1], 0, False), (f.tables[1][0], f.tables[1][1], 0, False),
+            (f.tables[0][0], f.tables[0][1], 0, False)]
+    return O.evaluate(req.spin.dimension, O.Field(9, tabs), [1.0, 1.0, 0.0, 0.0], req.time_start, req.time_end,
+                      req.time_step_integration, req.time_step_output, req.state_init)
+
+
+def requests(n=24, rate=2e5, seed=7, max_duration=400e-6):
+    from spinsim_b200.serving import synthetic_requests
+    return synthetic_requests(n, rate, seed=seed, max_duration=max_duration)
+
+
+def test_serving_fp64_matches_oracle_and_is_mix_independent(cuda):
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Server
+    reqs = requests()
+    srv = Server(precision=ss.Precision.FP64, streams=3, max_batch=6)
+    done = srv.run(reqs)
+    assert len(done) == len(reqs)
+    assert srv.stats["launches"] >= 4
+    by_id = {c.request.id: c for c in done}
+    for r in reqs[:10]:
+        t, u, s, sp = oracle_of(r)
+        got = by_id[r.id].results
+        assert np.array_equal(got.time, t)
+        assert np.abs(got.time_evolution - u).max() < 1e-10
+        assert np.abs(got.state - s).max() < 1e-10
+    for r in reqs[::5]:
+        alone = Server(precision=ss.Precision.FP64, streams=1).run([r])[0].results
+        assert np.array_equal(alone.state, by_id[r.id].results.state)
+        assert np.array_equal(alone.time_evolution, by_id[r.id].results.time_evolution)
+
+
+def test_serving_fp32_bulk_alone_equals_mix_and_error_bound(cuda):
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Server
+    reqs = requests(seed=8)
+    done = Server(precision=ss.Precision.FP32_BULK, streams=2, max_batch=5).run(reqs)
+    by_id = {c.request.id: c for c in done}
+    for r in reqs[::4]:
+        alone = Server(precision=ss.Precision.FP32_BULK, streams=1).run([r])[0].results
+        assert np.array_equal(alone.state, by_id[r.id].results.state)
+        t, u, s, sp = oracle_of(r)
+        assert np.abs(by_id[r.id].results.state - s).max() < 1e-6
+
+
+def test_hbm_budget_admission(cuda):
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Server
+    reqs = requests(n=12, rate=1e6, seed=9)
+    budget = max(r.footprint() for r in reqs) + 1
+    srv = Server(precision=ss.Precision.FP64, hbm_budget=budget, streams=4)
+    done = srv.run(reqs)
+    assert len(done) == len(reqs)
+    assert srv.stats["budget_waits"] > 0
+    with pytest.raises(ValueError):
+        Server(precision=ss.Precision.FP64, hbm_budget=1000).run(reqs[:1])
