@@ -274,6 +274,9 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     double bias[L];
 #pragma unroll
     for (int c = 0; c < L; c++) bias[c] = f.bias[c];
+    TableCursor cur[L];  // per-channel table cursors for the increasing sample times of the steps
+#pragma unroll
+    for (int c = 0; c < L; c++) cur[c] = TableCursor{-1, 0.0, 0.0};
 
     // ---- tone synthesis set-up (FIELD_TONES)
     ToneShared* ts = nullptr;
@@ -366,8 +369,8 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
                 s0[k] = 0.0;
                 s1[k] = 0.0;
             }
-            sample_field<FIELD, L>(f, t_fine + a_lo, s0);
-            sample_field<FIELD, L>(f, t_fine + a_hi, s1);
+            sample_field<FIELD, L>(f, t_fine + a_lo, s0, cur);
+            sample_field<FIELD, L>(f, t_fine + a_hi, s1, cur);
         }
         if (m.rotating) {  // xy times exp(-i P rw tau), z minus P rw
             const c64 Wn = W * Wrot;

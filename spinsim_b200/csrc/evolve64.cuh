@@ -99,6 +99,9 @@ SS_D void interval64(const MethodConfig& m, const Instance& inst, const FieldDes
 
     Mat<D> u;
     set_identity(u);
+    TableCursor cur[L];  // per-channel table cursors for the increasing sample times of the steps
+#pragma unroll
+    for (int c = 0; c < L; c++) cur[c] = TableCursor{-1, 0.0, 0.0};
     const double a_lo = 0.5 * dt * (1.0 - 1.0 / kSqrt3);
     const double a_hi = 0.5 * dt * (1.0 + 1.0 / kSqrt3);
     const double w0 = (1.5 + kSqrt3) / 6.0, w1 = (1.5 - kSqrt3) / 6.0;
@@ -111,7 +114,7 @@ SS_D void interval64(const MethodConfig& m, const Instance& inst, const FieldDes
             c64 wa = c64{1.0, 0.0};
             if (m.rotating) sincos(rw * ts, &wa.im, &wa.re);
             ts += t_c;
-            sample_field<FIELD, L>(f, ts, s0);
+            sample_field<FIELD, L>(f, ts, s0, cur);
             if (m.rotating) transform_frame64<D, EXPO>(s0, rw, wa);
             double g[L];
 #pragma unroll
@@ -128,11 +131,11 @@ SS_D void interval64(const MethodConfig& m, const Instance& inst, const FieldDes
             c64 wa = c64{1.0, 0.0}, wb = c64{1.0, 0.0};
             if (m.rotating) sincos(rw * ts, &wa.im, &wa.re);
             ts += t_c;
-            sample_field<FIELD, L>(f, ts, s0);
+            sample_field<FIELD, L>(f, ts, s0, cur);
             ts = (INTEG == INTEG_CF4) ? ((t_fine + a_hi) - t_c) : (t_fine + dt - t_c);
             if (m.rotating) sincos(rw * ts, &wb.im, &wb.re);
             ts += t_c;
-            sample_field<FIELD, L>(f, ts, s1);
+            sample_field<FIELD, L>(f, ts, s1, cur);
             if (m.rotating) {
                 transform_frame64<D, EXPO>(s0, rw, wa);
                 transform_frame64<D, EXPO>(s1, rw, wb);

@@ -53,17 +53,11 @@ SS_D int64_t table_find(const TableChannel& tb, double ts, double* u) {
     return idx;
 }
 
-// The sampler bodies of I:2065-2140.
-SS_D double table_sample(const TableChannel& tb, double ts) {
+// Interpolation given the interval index i and parameter u (the sampler bodies of I:2065-2140).
+SS_D double table_value(const TableChannel& tb, int64_t i, double u) {
     const double* time = tb.time;
     const double* amp = tb.amplitude;
     const int64_t size = tb.size;
-    if (!tb.zero_boundary) {
-        if (ts <= __ldg(time)) return __ldg(amp);
-        if (ts >= __ldg(time + size - 1)) return __ldg(amp + size - 1);
-    }
-    double u;
-    const int64_t i = table_find(tb, ts, &u);
     if (tb.order == 0) return i >= 0 ? __ldg(amp + i) : 0.0;
     if (!(i >= 0 && i + 1 < size)) return 0.0;
     const double a0 = __ldg(amp + i), a1 = __ldg(amp + i + 1);
@@ -90,10 +84,56 @@ SS_D double table_sample(const TableChannel& tb, double ts) {
     return a0 * (2 * u3 - 3 * u2 + 1) + a1 * (-2 * u3 + 3 * u2) + g_left * (u3 - 2 * u2 + u) + g_right * (u3 - u2);
 }
 
+// The sampler of I:2065-2140 with the reference's search.
+SS_D double table_sample(const TableChannel& tb, double ts) {
+    if (!tb.zero_boundary) {
+        if (ts <= __ldg(tb.time)) return __ldg(tb.amplitude);
+        if (ts >= __ldg(tb.time + tb.size - 1)) return __ldg(tb.amplitude + tb.size - 1);
+    }
+    double u;
+    const int64_t i = table_find(tb, ts, &u);
+    return table_value(tb, i, u);
+}
+
+// A per-lane cursor over one table for sample times that only increase (the fine steps of an
+// output interval).  The interval [time[i], time[i+1]] that holds a sample strictly inside it is
+// unique, so advancing the cursor finds the same index as the reference's search; a sample that
+// lands exactly on a table time (or outside the table) goes to the reference's search, which picks
+// among the touching intervals as the reference does.  Results are therefore identical to
+// table_sample; the cursor only removes the bisection's chain of dependent loads.
+struct TableCursor {
+    int64_t i;         // -1: not positioned
+    double t_lo, t_hi;
+};
+
+SS_D double table_sample_cursor(const TableChannel& tb, double ts, TableCursor& cur) {
+    if (!tb.zero_boundary) {
+        if (ts <= __ldg(tb.time)) return __ldg(tb.amplitude);
+        if (ts >= __ldg(tb.time + tb.size - 1)) return __ldg(tb.amplitude + tb.size - 1);
+    }
+    if (cur.i >= 0) {
+        while (ts >= cur.t_hi && cur.i + 2 < tb.size) {
+            cur.i++;
+            cur.t_lo = cur.t_hi;
+            cur.t_hi = __ldg(tb.time + cur.i + 1);
+        }
+        if (ts > cur.t_lo && ts < cur.t_hi) return table_value(tb, cur.i, (ts - cur.t_lo) / (cur.t_hi - cur.t_lo));
+    }
+    double u;
+    const int64_t i = table_find(tb, ts, &u);
+    if (i >= 0 && i + 1 < tb.size) {
+        cur.i = i;
+        cur.t_lo = __ldg(tb.time + i);
+        cur.t_hi = __ldg(tb.time + i + 1);
+    }
+    return table_value(tb, i, u);
+}
+
 // Sample the field at time t into out[0..NCH) (entries beyond NCH are left untouched).
-// The caller pre-zeroes `out` like the reference does before each sample (I:625-642).
+// The caller pre-zeroes `out` like the reference does before each sample (I:625-642).  `cursors`
+// (FIELD_TABLE, optional) hold one TableCursor per channel for increasing sample times.
 template <int FIELD, int NCH>
-SS_D void sample_field(const FieldDesc& f, double t, double* out) {
+SS_D void sample_field(const FieldDesc& f, double t, double* out, TableCursor* cursors = nullptr) {
     if constexpr (FIELD == FIELD_USER) {
 #ifdef SPINSIM_USER_FIELD
         spinsim_user_field(t, const_cast<double*>(f.params), f.n_params, out);
@@ -101,8 +141,13 @@ SS_D void sample_field(const FieldDesc& f, double t, double* out) {
     } else if constexpr (FIELD == FIELD_TABLE) {
 #pragma unroll
         for (int c = 0; c < NCH; c++) {
-            const TableChannel tb = f.tables[c];
-            out[c] = (tb.size > 0) ? fma(f.gain[c], table_sample(tb, t), f.bias[c]) : f.bias[c];
+            const TableChannel& tb = f.tables[c];
+            if (tb.size > 0) {
+                const double v = cursors ? table_sample_cursor(tb, t, cursors[c]) : table_sample(tb, t);
+                out[c] = fma(f.gain[c], v, f.bias[c]);
+            } else {
+                out[c] = f.bias[c];
+            }
         }
     } else {  // FIELD_TONES
 #pragma unroll
