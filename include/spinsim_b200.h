@@ -161,6 +161,18 @@ size_t spinsim_state_workspace_size(int32_t dim, int64_t n_out);
 int spinsim_state(int32_t dim, const double* u_dev, int64_t n_out, const double* psi0, double* state_dev,
                   double* spin_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
 
+/* spinsim_state without a workspace argument; no counterpart in the reference.  For callers that may
+ * not allocate device memory (a plugin that only receives buffers from a host application owning
+ * every allocation, or a loop that cannot afford cudaMalloc's device-wide synchronisation): the scan's
+ * scratch is a fixed array inside this library (5 MiB, held on every GPU that loads the library
+ * until exit).  At most spinsim_state_static_max_steps() output steps (262144); larger inputs are
+ * rejected with SPINSIM_ERR_INVALID.  The first call on a device looks up the array's device address
+ * (make it before any stream capture).  Calls share the array: calls whose work overlaps on the GPU
+ * race and must be serialised by the caller.  Allocates nothing. */
+int64_t spinsim_state_static_max_steps(void);
+int spinsim_state_static(int32_t dim, const double* u_dev, int64_t n_out, const double* psi0, double* state_dev,
+                         double* spin_dev, void* stream);
+
 /* get_spin alone (I:899-959; spin_calculator I:961-988): spin_dev[N][3] from state_dev[N][d]. */
 int spinsim_spin(int32_t dim, const double* state_dev, int64_t n_out, double* spin_dev, void* stream);
 

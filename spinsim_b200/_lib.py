@@ -86,6 +86,8 @@ _SIGNATURES = [
     ("spinsim_batch_launch", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("spinsim_batch_destroy", ctypes.c_int, [c_vp]),
     ("spinsim_fma_peak", ctypes.c_int, [c_i32, ctypes.POINTER(c_dbl), c_vp]),
+    ("spinsim_state_static_max_steps", c_i64, []),
+    ("spinsim_state_static", ctypes.c_int, [c_i32, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp]),
 ]
 
 EXPORTED = [name for name, _, _ in _SIGNATURES]
