@@ -73,9 +73,23 @@ def instances(ss, specs):
 
 
 # Algorithmic work per integration step, counted from the kernels' arithmetic (a fused multiply-add
-# is 2 flops; sin, cos, sqrt and division count 1 each).  See DESIGN.md, "Work per step".
+# is 2 flops; sin, cos, sqrt and division count 1 each).  Plain FP64, spin half: field 192 + 48 sin,
+# windings 8 + 4 sincos, frame 24, generators 24, two analytic exponentials 40 + 8, two 2x2 complex
+# products 128, time 1.  Spin one (Lie-Trotter, 24 squarings): field 192 + 48, windings 8 + 4,
+# frame 14, generators 32, two exponentials 10,920 + 14, two 3x3 products 432, time 1.  FP32-bulk:
+# tone synthesis 192 (two FMAs per tone and Gauss point) + producer share 9 + sums 6, frame 32,
+# generators 18 (24 for spin one), SU(2) product 32, time 1 in FP64; two SU(2) exponentials and their
+# product 90 in FP32.
 FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
-FLOPS_BULK = {2: {"fp64": 467, "fp32": 82}, 3: {"fp64": 467, "fp32": 82}}
+FLOPS_BULK = {2: {"fp64": 290, "fp32": 90}, 3: {"fp64": 296, "fp32": 90}}
+# DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload, from
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (1 pass), profiles/evolve_fp32bulk_tones.md.
+TRAFFIC_BYTES_PER_LAUNCH = 1853696 + 81376256
+
+
+def algorithmic_bytes(specs):
+    """Bytes one time-evolution launch must write: time (8) and U (16 d^2) per output step."""
+    return sum(int(dur / 1e-6) * (8 + 16 * dim * dim) for dim, dur, _ in specs)
 
 
 def algorithmic_flops(specs, form):
@@ -331,7 +345,8 @@ def bench_ours(args, world, rank):
         "state_err": {"max": float(errs.max()), "p50": float(np.median(errs)), "p99": float(np.percentile(errs, 99)),
                       "tolerance": 1e-6, "vs": "plain FP64 form, final state state[N-1] per instance"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak["tflops"], "unit": "TFLOP/s",
-                     "frac": achieved / fp64_peak["tflops"], "traffic": None,
+                     "frac": achieved / fp64_peak["tflops"], "traffic": TRAFFIC_BYTES_PER_LAUNCH,
+                     "algorithmic_bytes": algorithmic_bytes(specs),
                      "kernel": "spinsim::evolve_kernel (FP32-bulk, mixed dims, tones)",
                      "peak_source": fp64_peak["source"],
                      "fp32_achieved": fp32_flops / evolve_s / 1e12,
@@ -433,6 +448,85 @@ def bench_serving(args):
     return out
 
 
+def _event_time(fn, reps=3):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(reps):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    return best
+
+
+def bench_configs(args):
+    """The drop-in on the other reference workloads (plain FP64, and FP32-bulk where it applies):
+    Larmor precession (spin half, 200,000 output steps), the spin-one detuned Rabi sweep (64 detunings,
+    Lie-Trotter 28 squarings) and the spin-half Gaussian-pulse ensemble (4096 members)."""
+    import math
+    import torch
+    import spinsim_b200 as ss
+    from spinsim_b200.batch import Batch, Instance
+    import fields as F
+    out = {"metric": "steps/s per reference workload", "workload": "configs", "configs": {}}
+    # Larmor: one evaluate() through the drop-in API (FP64)
+    sim = ss.Simulator(F.larmor, ss.SpinQuantumNumber.HALF)
+    t = _event_time(lambda: sim.evaluate(0, 100e-3, 100e-9, 500e-9, ss.SpinQuantumNumber.HALF.plus_x))
+    out["configs"]["larmor_fp64"] = {"steps": 1_000_000, "seconds": t, "steps_per_s": 1e6 / t}
+    # detuned spin-one Rabi sweep: 64 instances of one user field
+    deltas = np.random.default_rng(seed=1).uniform(-5e3, 5e3, 64)
+    insts = [Instance(ss.SpinQuantumNumber.ONE, 0, 10e-3, 10e-9, 100e-9, ss.SpinQuantumNumber.ONE.plus_z, [d])
+             for d in deltas]
+    res = {}
+    for prec in (ss.Precision.FP64, ss.Precision.FP32_BULK):
+        b = Batch(insts, get_field=F.detuned_rabi, number_of_squares=28, precision=prec,
+                  max_registers=128 if prec == ss.Precision.FP64 else 0)
+        tt = _event_time(b.run, reps=2)
+        res[prec.name] = b
+        out["configs"][f"detuned_rabi_{prec.name.lower()}"] = {"steps": b.total_steps, "seconds": tt,
+                                                              "steps_per_s": b.total_steps / tt}
+    e = np.array([np.abs(x - y).max() for x, y in zip(res["FP32_BULK"].final_states(), res["FP64"].final_states())])
+    out["configs"]["detuned_rabi_fp32_bulk"]["state_err_max"] = float(e.max())
+    # Gaussian-pulse ensemble: 4096 members
+    members = np.random.default_rng(seed=2).normal(0.0, 500.0, 4096)
+    insts = [Instance(ss.SpinQuantumNumber.HALF, 0, 1e-3, 20e-9, 1e-6, ss.SpinQuantumNumber.HALF.plus_z, [m])
+             for m in members]
+    res = {}
+    for prec in (ss.Precision.FP64, ss.Precision.FP32_BULK):
+        b = Batch(insts, get_field=F.gaussian_ensemble, precision=prec)
+        tt = _event_time(b.run, reps=2)
+        res[prec.name] = b
+        out["configs"][f"gaussian_ensemble_{prec.name.lower()}"] = {"steps": b.total_steps, "seconds": tt,
+                                                                   "steps_per_s": b.total_steps / tt}
+    e = np.array([np.abs(x - y).max() for x, y in zip(res["FP32_BULK"].final_states(), res["FP64"].final_states())])
+    out["configs"]["gaussian_ensemble_fp32_bulk"].update({"state_err_max": float(e.max()),
+                                                          "state_err_p50": float(np.median(e))})
+    _ = math
+    return out
+
+
+def profile_case(args):
+    """One launch of the benchmark batch for profilers: the full batch, or a small case (the first 256
+    instances with durations capped at 1 ms) that a full ncu capture can replay quickly."""
+    import torch
+    import spinsim_b200 as ss
+    from spinsim_b200.batch import Batch
+    specs = workload()
+    if args.profile_size == "small":
+        specs = [(d, min(t, 1e-3), p) for d, t, p in specs[:256]]
+    prec = ss.Precision.FP32_BULK if args.precision == "fp32_bulk" else ss.Precision.FP64
+    b = Batch(instances(ss, specs), precision=prec, max_registers=args.max_registers, lanes=args.lanes)
+    b.run(with_state=not args.evolve_only)
+    torch.cuda.synchronize()
+    return {"workload": f"profile-{args.profile_size}", "precision": args.precision, "steps": b.total_steps,
+            "intervals": b.n_intervals, "plan": b.plan_info()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -440,7 +534,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="batch", choices=["batch", "serving"])
+    ap.add_argument("--workload", default="batch", choices=["batch", "serving", "configs", "profile"])
+    ap.add_argument("--profile-size", default="small", choices=["small", "full"])
+    ap.add_argument("--precision", default="fp32_bulk", choices=["fp32_bulk", "fp64"])
+    ap.add_argument("--max-registers", type=int, default=168)
+    ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--evolve-only", action="store_true")
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--streams", type=int, default=4)
@@ -460,6 +559,13 @@ def main():
     if args.workload == "serving":
         if rank == 0:
             print(json.dumps(bench_serving(args)), flush=True)
+        return
+    if args.workload == "profile":
+        print(json.dumps(profile_case(args)), flush=True)
+        return
+    if args.workload == "configs":
+        if rank == 0:
+            print(json.dumps(bench_configs(args)), flush=True)
         return
     out, specs = bench_ours(args, world, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -72,7 +72,7 @@ class Server:
     on up to ``streams`` concurrent launches of at most ``max_batch`` requests each."""
 
     def __init__(self, precision=Precision.FP32_BULK, hbm_budget=8 << 30, streams=4, max_batch=4096,
-                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=0):
+                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=128):
         import torch
         self.precision = Precision(precision)
         self.hbm_budget = int(hbm_budget)
