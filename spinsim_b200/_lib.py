@@ -8,7 +8,7 @@ import os
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libspinsim_b200.so")
+LIB_PATH = os.environ.get("SPINSIM_LIB", os.path.join(HERE, "libspinsim_b200.so"))
 
 OK = 0
 ERR_INVALID = -1

@@ -21,6 +21,11 @@
 #include "common.cuh"
 #include "evolve64.cuh"
 
+// 1: the next step's field samples are issued next to this step's exponentials (software pipeline).
+#ifndef SPINSIM_BULK_PIPELINE
+#define SPINSIM_BULK_PIPELINE 1
+#endif
+
 namespace spinsim {
 
 struct c32 {
@@ -216,17 +221,9 @@ SS_D void su2_apply(Su2d& p, const Su2f& e) {
     p.beta = nb;
 }
 
-// ---------------------------------------------------------------------------------- tone synthesis
-// Warp-cooperative evaluation of tone fields (FIELD_TONES).  The 32 lanes of a warp work on
-// consecutive output intervals of one instance and step through their fine steps in lockstep, so
-// the sample times differ between lanes only by the interval start t_c.  Writing
-//     A sin(w (t_c + tau) + phi) = Im( L(t_c) U(tau) ),  L = A exp(i (w t_c + phi)),  U = exp(i w tau),
-// each lane keeps its L for the interval in shared memory (read-only), while U(tau) for the current
-// step is the same for the whole warp: lane k advances tone k's U by an FP64 recurrence
-// (U <- U exp(i w dt)) and publishes it, with V = U exp(i w (a_hi - a_lo)) for the second Gauss
-// point, through a double-buffered shared slot.  Per lane and tone a sample then costs two FMAs.
-static_assert(sizeof(ToneShared) == kToneSharedBytes, "tone shared layout");
-
+// ---------------------------------------------------------------------------------- generic bulk path
+// One output interval per lane (USER and TABLE fields, and tone fields the synthesis below does not
+// take: spin one with a quadratic shift).
 template <int D, int INTEG, int EXPO, int FIELD>
 SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDesc& f, int64_t index, bool active,
                      int lane_in_group, double* time_out, double* u_out) {
@@ -234,8 +231,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     static_assert(EXPO != EXPO_LIE_TROTTER_8, "the FP32-bulk form has no eight-generator exponential");
     constexpr int L = (D == 2) ? 3 : 4;
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
-    constexpr bool TONES = (FIELD == FIELD_TONES);
-    const int lanes = TONES ? 1 : m.lanes;  // tone synthesis runs the warp's lanes in lockstep
+    const int lanes = m.lanes;
     const double dt = inst.dt_int, dt_out = inst.dt_out;
     const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)index));  // I:818, unfused
     double s0[8], s1[8];
@@ -250,9 +246,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         rw = s0[2];
         if (D == 2) rw /= 2;
     }
-    // With tone synthesis every lane of the warp runs the instance's K steps (inactive lanes only
-    // publish tone phasors); otherwise inactive lanes run none.
-    const int K = (active || TONES) ? inst.n_fine : 0;
+    const int K = active ? inst.n_fine : 0;
     const int j0 = (int)(((int64_t)K * lane_in_group) / lanes);
     const int j1 = (int)(((int64_t)K * (lane_in_group + 1)) / lanes);
     double t_fine = t_c;
@@ -270,108 +264,19 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         sincos(-(double)P * rw * dt, &Wrot.im, &Wrot.re);
         sincos(-(double)P * rw * a_lo, &Woff.im, &Woff.re);
     }
-
-    double bias[L];
-#pragma unroll
-    for (int c = 0; c < L; c++) bias[c] = f.bias[c];
     TableCursor cur[L];  // per-channel table cursors for the increasing sample times of the steps
 #pragma unroll
     for (int c = 0; c < L; c++) cur[c] = TableCursor{-1, 0.0, 0.0};
 
-    // ---- tone synthesis set-up (FIELD_TONES)
-    ToneShared* ts = nullptr;
-    const int lane = threadIdx.x & 31;
-    c64 u_prod = c64{0.0, 0.0}, u_rot = c64{1.0, 0.0}, u_gap = c64{1.0, 0.0};
-    bool direct_tones = false;  // tones beyond kBulkTones on x, y, z, or any tone on q
-    if constexpr (TONES) {
-        extern __shared__ __align__(16) unsigned char spinsim_dyn_smem[];
-        ts = reinterpret_cast<ToneShared*>(spinsim_dyn_smem) + (threadIdx.x >> 5);
-#pragma unroll
-        for (int c = 0; c < L; c++) direct_tones |= f.tone_count[c] > (c < 3 ? kBulkTones : 0);
-        // this lane's L for every slot
-#pragma unroll 1
-        for (int slot = 0; slot < kToneSlots; slot++) {
-            const int c = slot / kBulkTones, k = slot % kBulkTones;
-            double re = 0.0, im = 0.0;
-            if (active && k < f.tone_count[c]) {
-                const double* tone = f.tones + 3 * (f.tone_start[c] + k);
-                const double amp = f.gain[c] * __ldg(tone + 1);
-                double sn, cs;
-                sincos(fma(__ldg(tone), t_c, __ldg(tone + 2)), &sn, &cs);
-                re = amp * cs;
-                im = amp * sn;
-            }
-            ts->l[slot][lane][0] = re;
-            ts->l[slot][lane][1] = im;
-        }
-        // producer lane `lane` owns slot `lane`: U(a_lo), rotation per step, gap to a_hi
-        if (lane < kToneSlots) {
-            const int c = lane / kBulkTones, k = lane % kBulkTones;
-            if (k < f.tone_count[c]) {
-                const double w = __ldg(f.tones + 3 * (f.tone_start[c] + k));
-                sincos(w * a_lo, &u_prod.im, &u_prod.re);
-                sincos(w * dt, &u_rot.im, &u_rot.re);
-                sincos(w * (a_hi - a_lo), &u_gap.im, &u_gap.re);
-            }
-        }
-    }
-
     // One step's field samples (FP64) -> frame transform -> CF4 generators rounded to FP32.
-    auto step_generators = [&](int j, float* ga, float* gb) {
-        if constexpr (TONES) {
-            // publish U, V of step j, then read them back for every slot
-            if (lane < kToneSlots) {
-                const c64 v = u_prod * u_gap;
-                double* dst = ts->uv[j & 1][lane];
-                dst[0] = u_prod.re;
-                dst[1] = u_prod.im;
-                dst[2] = v.re;
-                dst[3] = v.im;
-                u_prod = u_prod * u_rot;
-            }
-            __syncwarp();
+    auto step_generators = [&](float* ga, float* gb) {
 #pragma unroll
-            for (int c = 0; c < L; c++) {
-                double acc_a = bias[c], acc_b = bias[c];
-                if (c < 3) {
-                    double pa = 0.0, pb = 0.0;
-#pragma unroll
-                    for (int k = 0; k < kBulkTones; k++) {
-                        const int slot = c * kBulkTones + k;
-                        const double2 lv = *reinterpret_cast<const double2*>(ts->l[slot][lane]);
-                        const double2 uu = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][0]);
-                        const double2 vv = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][2]);
-                        if (k & 1) {
-                            pa = fma(lv.x, uu.y, fma(lv.y, uu.x, pa));
-                            pb = fma(lv.x, vv.y, fma(lv.y, vv.x, pb));
-                        } else {
-                            acc_a = fma(lv.x, uu.y, fma(lv.y, uu.x, acc_a));
-                            acc_b = fma(lv.x, vv.y, fma(lv.y, vv.x, acc_b));
-                        }
-                    }
-                    acc_a += pa;
-                    acc_b += pb;
-                }
-                if (direct_tones) {  // tones past the synthesis slots, and the q channel
-                    for (int k = (c < 3 ? kBulkTones : 0); k < f.tone_count[c]; k++) {
-                        const double* tone = f.tones + 3 * (f.tone_start[c] + k);
-                        const double w = __ldg(tone), a = f.gain[c] * __ldg(tone + 1), ph = __ldg(tone + 2);
-                        acc_a = fma(a, sin(fma(w, t_fine + a_lo, ph)), acc_a);
-                        acc_b = fma(a, sin(fma(w, t_fine + a_hi, ph)), acc_b);
-                    }
-                }
-                s0[c] = acc_a;
-                s1[c] = acc_b;
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < L; k++) {
-                s0[k] = 0.0;
-                s1[k] = 0.0;
-            }
-            sample_field<FIELD, L>(f, t_fine + a_lo, s0, cur);
-            sample_field<FIELD, L>(f, t_fine + a_hi, s1, cur);
+        for (int k = 0; k < L; k++) {
+            s0[k] = 0.0;
+            s1[k] = 0.0;
         }
+        sample_field<FIELD, L>(f, t_fine + a_lo, s0, cur);
+        sample_field<FIELD, L>(f, t_fine + a_hi, s1, cur);
         if (m.rotating) {  // xy times exp(-i P rw tau), z minus P rw
             const c64 Wn = W * Wrot;
             const c64 xa = c64{s0[0], s0[1]} * (W * Woff);
@@ -398,24 +303,17 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     float ga[4] = {0.0f, 0.0f, 0.0f, 0.0f}, gb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     int j = j0;
     bool pending = false;
-    if (j < j1) step_generators(j, ga, gb);
+    if (j < j1) step_generators(ga, gb);
     for (; j < j1; j++) {
-        if constexpr (D == 3 && !TONES) {
+        if constexpr (D == 3) {
             if (ga[3] != 0.0f || gb[3] != 0.0f) {
-                pending = true;
-                break;
-            }
-        }
-        if constexpr (D == 3 && TONES) {
-            // the whole warp leaves phase 1 together (tone synthesis is in lockstep)
-            if (__any_sync(0xffffffffu, active && (ga[3] != 0.0f || gb[3] != 0.0f))) {
                 pending = true;
                 break;
             }
         }
         float na[4] = {0.0f, 0.0f, 0.0f, 0.0f}, nb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         t_fine += dt;
-        if (j + 1 < j1) step_generators(j + 1, na, nb);
+        if (j + 1 < j1) step_generators(na, nb);
         su2_apply(su2, su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2])));
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -436,11 +334,12 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         }
     }
     // Phase 2 (spin one with a quadratic shift): full 3x3 exponentials and an FP64 3x3 product.
+    // On entry t_fine is the pending step's start and its generators are in ga, gb.
     if constexpr (D == 3) {
         if (pending) {
             bool first = true;
             for (; j < j1; j++) {
-                if (!first) step_generators(j, ga, gb);
+                if (!first) step_generators(ga, gb);
                 first = false;
                 const Mat32<3> ea = spin_one_exp_m1(ga[0], ga[1], ga[2], ga[3]);
                 const Mat32<3> eb = spin_one_exp_m1(gb[0], gb[1], gb[2], gb[3]);
@@ -449,7 +348,6 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             }
         }
     }
-    if constexpr (TONES) __syncwarp();  // the shared slots are reused by the warp's next tile
 
     for (int s = 1; s < lanes; s <<= 1) {
         const Mat<D> later = shfl_down_mat(u, s);
@@ -472,6 +370,220 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     for (int i = 0; i < D; i++)
 #pragma unroll
         for (int k = 0; k < D; k++) dst[i * D + k] = make_double2(u.a[i][k].re, u.a[i][k].im);
+}
+
+// ---------------------------------------------------------------------------------- tone synthesis
+// Warp-cooperative evaluation of tone fields (FIELD_TONES, no quadratic shift).  A warp takes a
+// tile of 32 * kSynthIntervals consecutive output intervals of one instance; lane l works on
+// intervals l, l + 32, ...; every lane steps through the instance's K fine steps in lockstep, so
+// the sample times differ between intervals only by the interval start t_c.  Writing
+//     A sin(w (t_c + tau) + phi) = Im( L(t_c) U(tau) ),  L = A exp(i (w t_c + phi)),  U = exp(i w tau),
+// each interval keeps its L in shared memory (read-only for the interval), while U(tau) for the
+// current step is the same for the whole warp: lane k advances tone k's U by an FP64 recurrence
+// (U <- U exp(i w dt)) and publishes it, with V = U exp(i w (a_hi - a_lo)) for the second Gauss
+// point, through a double-buffered shared slot.  A sample then costs two FMAs per tone; one U, V
+// load serves all of a lane's intervals, and the intervals' dependent chains interleave.
+extern __shared__ __align__(16) unsigned char spinsim_dyn_smem[];
+static_assert(sizeof(ToneShared) == kToneSharedBytes, "tone shared layout");
+
+SS_D bool tones_have_quadratic_shift(const FieldDesc& f) { return f.bias[3] != 0.0 || f.tone_count[3] > 0; }
+
+template <int D, int EXPO>
+SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const FieldDesc& f, const Tile& tile,
+                            double* time_out, double* u_out) {
+    constexpr int NI = kSynthIntervals;
+    constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
+    const int lane = threadIdx.x & 31;
+    ToneShared* ts = reinterpret_cast<ToneShared*>(spinsim_dyn_smem) + (threadIdx.x >> 5);
+    const double dt = inst.dt_int, dt_out = inst.dt_out;
+    const int K = inst.n_fine;
+    const double a_lo = 0.5 * dt * (1.0 - 1.0 / kSqrt3);
+    const double a_hi = 0.5 * dt * (1.0 + 1.0 / kSqrt3);
+    const double w0 = (1.5 + kSqrt3) / 6.0, w1 = (1.5 - kSqrt3) / 6.0;
+    const double c0 = dt * w0, c1 = dt * w1;
+
+    bool active[NI];
+    int64_t index[NI];
+    double t_c[NI], rw[NI];
+    c64 W[NI], Wrot[NI], Woff[NI];
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        active[i] = lane + 32 * i < tile.count;
+        index[i] = tile.first + (active[i] ? lane + 32 * i : 0);
+        t_c[i] = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)index[i]));  // I:818, unfused
+        rw[i] = 0.0;
+        W[i] = Wrot[i] = Woff[i] = c64{1.0, 0.0};
+        if (active[i] && m.rotating) {
+            double smp[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            sample_field<FIELD_TONES, 3>(f, t_c[i] + dt_out / 2, smp);
+            rw[i] = (D == 2) ? smp[2] / 2 : smp[2];
+            sincos(-(double)P * rw[i] * dt, &Wrot[i].im, &Wrot[i].re);
+            sincos(-(double)P * rw[i] * a_lo, &Woff[i].im, &Woff[i].re);
+        }
+    }
+    bool direct = false;  // tones past the synthesis slots (sampled directly)
+    double bias[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        direct |= f.tone_count[c] > kBulkTones;
+        bias[c] = f.bias[c];
+    }
+    // L of every slot and interval; the producer constants of slot `lane`
+#pragma unroll 1
+    for (int slot = 0; slot < kToneSlots; slot++) {
+        const int c = slot / kBulkTones, k = slot % kBulkTones;
+        double w = 0.0, amp = 0.0, ph = 0.0;
+        const bool on = k < f.tone_count[c];
+        if (on) {
+            const double* tone = f.tones + 3 * (f.tone_start[c] + k);
+            w = __ldg(tone);
+            amp = f.gain[c] * __ldg(tone + 1);
+            ph = __ldg(tone + 2);
+        }
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+            double sn = 0.0, cs = 0.0;
+            if (on && active[i]) sincos(fma(w, t_c[i], ph), &sn, &cs);
+            ts->l[slot][i][lane][0] = amp * cs;
+            ts->l[slot][i][lane][1] = amp * sn;
+        }
+    }
+    c64 u_prod = c64{0.0, 0.0};
+    if (lane < kToneSlots) {
+        const int c = lane / kBulkTones, k = lane % kBulkTones;
+        double rg[4] = {1.0, 0.0, 1.0, 0.0};
+        if (k < f.tone_count[c]) {
+            const double w = __ldg(f.tones + 3 * (f.tone_start[c] + k));
+            sincos(w * a_lo, &u_prod.im, &u_prod.re);
+            sincos(w * dt, &rg[1], &rg[0]);
+            sincos(w * (a_hi - a_lo), &rg[3], &rg[2]);
+        }
+        ts->rg[lane][0] = rg[0];
+        ts->rg[lane][1] = rg[1];
+        ts->rg[lane][2] = rg[2];
+        ts->rg[lane][3] = rg[3];
+    }
+
+    Su2d su2[NI];
+#pragma unroll
+    for (int i = 0; i < NI; i++) su2[i] = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
+    for (int j = 0; j < K; j++) {
+        // publish U, V of step j
+        if (lane < kToneSlots) {
+            const double2 rot = *reinterpret_cast<const double2*>(&ts->rg[lane][0]);
+            const double2 gap = *reinterpret_cast<const double2*>(&ts->rg[lane][2]);
+            const c64 v = u_prod * c64{gap.x, gap.y};
+            double* dst = ts->uv[j & 1][lane];
+            dst[0] = u_prod.re;
+            dst[1] = u_prod.im;
+            dst[2] = v.re;
+            dst[3] = v.im;
+            u_prod = u_prod * c64{rot.x, rot.y};
+        }
+        __syncwarp();
+        // field samples at the two Gauss points of every interval (FP64)
+        double sa[NI][3], sb[NI][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double pa[NI], pb[NI];
+#pragma unroll
+            for (int i = 0; i < NI; i++) {
+                sa[i][c] = bias[c];
+                sb[i][c] = bias[c];
+                pa[i] = 0.0;
+                pb[i] = 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < kBulkTones; k++) {
+                const int slot = c * kBulkTones + k;
+                const double2 uu = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][0]);
+                const double2 vv = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][2]);
+#pragma unroll
+                for (int i = 0; i < NI; i++) {
+                    const double2 lv = *reinterpret_cast<const double2*>(ts->l[slot][i][lane]);
+                    if (k & 1) {
+                        pa[i] = fma(lv.x, uu.y, fma(lv.y, uu.x, pa[i]));
+                        pb[i] = fma(lv.x, vv.y, fma(lv.y, vv.x, pb[i]));
+                    } else {
+                        sa[i][c] = fma(lv.x, uu.y, fma(lv.y, uu.x, sa[i][c]));
+                        sb[i][c] = fma(lv.x, vv.y, fma(lv.y, vv.x, sb[i][c]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NI; i++) {
+                sa[i][c] += pa[i];
+                sb[i][c] += pb[i];
+            }
+            if (direct) {
+#pragma unroll
+                for (int i = 0; i < NI; i++) {
+                    const double t_step = t_c[i] + (double)j * dt;
+                    for (int k = kBulkTones; k < f.tone_count[c]; k++) {
+                        const double* tone = f.tones + 3 * (f.tone_start[c] + k);
+                        const double w = __ldg(tone), a = f.gain[c] * __ldg(tone + 1), ph = __ldg(tone + 2);
+                        sa[i][c] = fma(a, sin(fma(w, t_step + a_lo, ph)), sa[i][c]);
+                        sb[i][c] = fma(a, sin(fma(w, t_step + a_hi, ph)), sb[i][c]);
+                    }
+                }
+            }
+        }
+        // frame transform, CF4 generators (rounded once to FP32), SU(2) exponentials and product
+#pragma unroll
+        for (int i = 0; i < NI; i++) {
+            if (m.rotating) {
+                const c64 Wn = W[i] * Wrot[i];
+                const c64 xa = c64{sa[i][0], sa[i][1]} * (W[i] * Woff[i]);
+                const c64 xb = c64{sb[i][0], sb[i][1]} * (Wn * conj(Woff[i]));
+                sa[i][0] = xa.re;
+                sa[i][1] = xa.im;
+                sb[i][0] = xb.re;
+                sb[i][1] = xb.im;
+                sa[i][2] -= (double)P * rw[i];
+                sb[i][2] -= (double)P * rw[i];
+                W[i] = Wn;
+            }
+            float ga[3], gb[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                ga[c] = __double2float_rn(fma(c0, sa[i][c], c1 * sb[i][c]));
+                gb[c] = __double2float_rn(fma(c1, sa[i][c], c0 * sb[i][c]));
+            }
+            su2_apply(su2[i], su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2])));
+        }
+    }
+    __syncwarp();  // the shared slots are reused by the warp's next tile
+
+#pragma unroll
+    for (int i = 0; i < NI; i++) {
+        if (!active[i]) continue;
+        const c64 alpha = c64{1.0 + su2[i].am1.re, su2[i].am1.im};
+        Mat<D> u;
+        if constexpr (D == 3) {
+            u = su2_to_spin_one(alpha, su2[i].beta);
+        } else {
+            u.a[0][0] = alpha;
+            u.a[1][0] = su2[i].beta;
+            u.a[0][1] = c64{-su2[i].beta.re, su2[i].beta.im};
+            u.a[1][1] = conj(alpha);
+        }
+        if (m.rotating) {  // leave the rotating frame, I:839-852
+            c64 wo;
+            sincos(rw[i] * dt_out, &wo.im, &wo.re);
+            const c64 woc = conj(wo);
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                u.a[0][k] = u.a[0][k] * woc;
+                u.a[D - 1][k] = u.a[D - 1][k] * wo;
+            }
+        }
+        time_out[index[i]] = t_c[i];
+        double2* dst = reinterpret_cast<double2*>(u_out) + index[i] * (D * D);
+#pragma unroll
+        for (int r = 0; r < D; r++)
+#pragma unroll
+            for (int k = 0; k < D; k++) dst[r * D + k] = make_double2(u.a[r][k].re, u.a[r][k].im);
+    }
 }
 
 }  // namespace spinsim

@@ -16,11 +16,14 @@ namespace spinsim {
 
 template <int DIMS, int INTEG, int EXPO_H, int EXPO_O, int FIELD, int PREC>
 SS_D void evolve_body(const EvolveArgs& a) {
+    // FP32-bulk tone fields are synthesised per warp: every lane takes kSynthIntervals intervals
+    // (the host sets lanes = 1 for these plans).
+    constexpr bool SYNTH = (PREC == PREC_FP32_BULK && FIELD == FIELD_TONES);
     const int lane = threadIdx.x & 31;
     const int lanes = a.m.lanes;
     const int group = lane / lanes;
     const int lane_in_group = lane - group * lanes;
-    const int per_warp = 32 / lanes;
+    const int per_warp = (SYNTH ? 32 * kSynthIntervals : 32) / lanes;
     const int64_t warp_global = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int64_t tile_id = warp_global;
     for (;;) {
@@ -42,22 +45,37 @@ SS_D void evolve_body(const EvolveArgs& a) {
         }
         const Instance& inst = a.instances[tile.instance];
         const FieldDesc& f = a.fields[inst.field];
-        const bool active = group < tile.count;
-        const int64_t index = tile.first + (active ? group : 0);
         double* time_out = a.time + inst.out_offset;
+        double* u_out = a.u + inst.u_offset;
         const int dim = (DIMS == 0) ? inst.dim : DIMS;
-        if (DIMS != 3 && dim == 2) {
-            double* u_out = a.u + inst.u_offset;
-            if constexpr (PREC == PREC_FP64)
-                interval64<2, INTEG, EXPO_H, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
-            else
-                interval32<2, INTEG, EXPO_H, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
-        } else if (DIMS != 2) {
-            double* u_out = a.u + inst.u_offset;
-            if constexpr (PREC == PREC_FP64)
-                interval64<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
-            else
-                interval32<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
+        if constexpr (SYNTH) {
+            if (DIMS != 2 && dim == 3 && tones_have_quadratic_shift(f)) {
+                // spin one with a quadratic shift: 3x3 exponentials, tones sampled directly
+#pragma unroll 1
+                for (int i = 0; i < kSynthIntervals; i++) {
+                    const bool act = lane + 32 * i < tile.count;
+                    const int64_t idx = tile.first + (act ? lane + 32 * i : 0);
+                    interval32<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, idx, act, 0, time_out, u_out);
+                }
+            } else if (DIMS != 3 && dim == 2) {
+                intervals32_synth<2, EXPO_H>(a.m, inst, f, tile, time_out, u_out);
+            } else if (DIMS != 2) {
+                intervals32_synth<3, EXPO_O>(a.m, inst, f, tile, time_out, u_out);
+            }
+        } else {
+            const bool active = group < tile.count;
+            const int64_t index = tile.first + (active ? group : 0);
+            if (DIMS != 3 && dim == 2) {
+                if constexpr (PREC == PREC_FP64)
+                    interval64<2, INTEG, EXPO_H, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
+                else
+                    interval32<2, INTEG, EXPO_H, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
+            } else if (DIMS != 2) {
+                if constexpr (PREC == PREC_FP64)
+                    interval64<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
+                else
+                    interval32<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
+            }
         }
         if (a.tile_counter == nullptr) return;
     }
