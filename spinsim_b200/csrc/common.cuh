@@ -105,13 +105,14 @@ struct EvolveArgs {
 // Shared memory of the FP32-bulk tone kernels (see evolve32.cuh), per warp.
 constexpr int kBulkTones = 8;               // tones per channel (x, y, z) synthesised per warp
 constexpr int kToneSlots = 3 * kBulkTones;  // slot = channel * kBulkTones + tone
-constexpr int kSynthIntervals = 2;          // output intervals per lane
+constexpr int kSynthIntervals = 2;          // output intervals per lane, 32 intervals apart
 struct ToneShared {
-    double l[kToneSlots][kSynthIntervals][32][2];  // [slot][interval][lane] (re, im) of L
-    double uv[2][kToneSlots][4];                   // [buffer][slot] U.re, U.im, V.re, V.im of the step
-    double rg[kToneSlots][4];                      // [slot] exp(i w dt), exp(i w (a_hi - a_lo))
+    double l[kToneSlots][32][2];                    // [slot][lane] (re, im) of L for the lane's first interval
+    double uv[2][kToneSlots][kSynthIntervals][4];   // [buffer][slot][interval] G^i U, G^i V of the step
+    double rg[kToneSlots][6];                       // [slot] exp(i w dt), exp(i w (a_hi - a_lo)), G
 };
-constexpr int kToneSharedBytes = kToneSlots * kSynthIntervals * 32 * 2 * 8 + 2 * kToneSlots * 4 * 8 + kToneSlots * 4 * 8;
+constexpr int kToneSharedBytes =
+    kToneSlots * 32 * 2 * 8 + 2 * kToneSlots * kSynthIntervals * 4 * 8 + kToneSlots * 6 * 8;
 
 // ------------------------------------------------------------------ complex helpers (FP64)
 struct c64 {

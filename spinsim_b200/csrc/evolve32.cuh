@@ -378,11 +378,12 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
 // intervals l, l + 32, ...; every lane steps through the instance's K fine steps in lockstep, so
 // the sample times differ between intervals only by the interval start t_c.  Writing
 //     A sin(w (t_c + tau) + phi) = Im( L(t_c) U(tau) ),  L = A exp(i (w t_c + phi)),  U = exp(i w tau),
-// each interval keeps its L in shared memory (read-only for the interval), while U(tau) for the
-// current step is the same for the whole warp: lane k advances tone k's U by an FP64 recurrence
-// (U <- U exp(i w dt)) and publishes it, with V = U exp(i w (a_hi - a_lo)) for the second Gauss
-// point, through a double-buffered shared slot.  A sample then costs two FMAs per tone; one U, V
-// load serves all of a lane's intervals, and the intervals' dependent chains interleave.
+// each lane keeps L of its first interval in shared memory (read-only for the tile); its interval
+// 32 i later has L G^i with G = exp(i w 32 dt_out), the same for the whole warp.  U(tau) for the
+// current step is also the same for the whole warp: lane k advances tone k's U by an FP64 recurrence
+// (U <- U exp(i w dt)) and publishes G^i U and G^i V, V = U exp(i w (a_hi - a_lo)) for the second
+// Gauss point, through a double-buffered shared slot.  A sample then costs two FMAs per tone and
+// interval; the intervals' dependent chains interleave.
 extern __shared__ __align__(16) unsigned char spinsim_dyn_smem[];
 static_assert(sizeof(ToneShared) == kToneSharedBytes, "tone shared layout");
 
@@ -428,57 +429,61 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
         direct |= f.tone_count[c] > kBulkTones;
         bias[c] = f.bias[c];
     }
-    // L of every slot and interval; the producer constants of slot `lane`
+    // L of every slot for the lane's first interval; the producer constants of slot `lane`
 #pragma unroll 1
     for (int slot = 0; slot < kToneSlots; slot++) {
         const int c = slot / kBulkTones, k = slot % kBulkTones;
-        double w = 0.0, amp = 0.0, ph = 0.0;
-        const bool on = k < f.tone_count[c];
-        if (on) {
+        double re = 0.0, im = 0.0;
+        if (k < f.tone_count[c]) {
             const double* tone = f.tones + 3 * (f.tone_start[c] + k);
-            w = __ldg(tone);
-            amp = f.gain[c] * __ldg(tone + 1);
-            ph = __ldg(tone + 2);
+            const double amp = f.gain[c] * __ldg(tone + 1);
+            double sn, cs;
+            sincos(fma(__ldg(tone), t_c[0], __ldg(tone + 2)), &sn, &cs);
+            re = amp * cs;
+            im = amp * sn;
         }
-#pragma unroll
-        for (int i = 0; i < NI; i++) {
-            double sn = 0.0, cs = 0.0;
-            if (on && active[i]) sincos(fma(w, t_c[i], ph), &sn, &cs);
-            ts->l[slot][i][lane][0] = amp * cs;
-            ts->l[slot][i][lane][1] = amp * sn;
-        }
+        ts->l[slot][lane][0] = re;
+        ts->l[slot][lane][1] = im;
     }
     c64 u_prod = c64{0.0, 0.0};
     if (lane < kToneSlots) {
         const int c = lane / kBulkTones, k = lane % kBulkTones;
-        double rg[4] = {1.0, 0.0, 1.0, 0.0};
+        double rg[6] = {1.0, 0.0, 1.0, 0.0, 1.0, 0.0};
         if (k < f.tone_count[c]) {
             const double w = __ldg(f.tones + 3 * (f.tone_start[c] + k));
             sincos(w * a_lo, &u_prod.im, &u_prod.re);
             sincos(w * dt, &rg[1], &rg[0]);
             sincos(w * (a_hi - a_lo), &rg[3], &rg[2]);
+            // G = exp(i w (t_c(l + 32) - t_c(l))), t_c rounded as the intervals' own starts are
+            sincos(w * (__dmul_rn(dt_out, (double)(index[0] + 32)) - __dmul_rn(dt_out, (double)index[0])),
+                   &rg[5], &rg[4]);
         }
-        ts->rg[lane][0] = rg[0];
-        ts->rg[lane][1] = rg[1];
-        ts->rg[lane][2] = rg[2];
-        ts->rg[lane][3] = rg[3];
+#pragma unroll
+        for (int q = 0; q < 6; q++) ts->rg[lane][q] = rg[q];
     }
 
     Su2d su2[NI];
 #pragma unroll
     for (int i = 0; i < NI; i++) su2[i] = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
     for (int j = 0; j < K; j++) {
-        // publish U, V of step j
+        // publish G^i U, G^i V of step j
         if (lane < kToneSlots) {
-            const double2 rot = *reinterpret_cast<const double2*>(&ts->rg[lane][0]);
-            const double2 gap = *reinterpret_cast<const double2*>(&ts->rg[lane][2]);
-            const c64 v = u_prod * c64{gap.x, gap.y};
-            double* dst = ts->uv[j & 1][lane];
-            dst[0] = u_prod.re;
-            dst[1] = u_prod.im;
-            dst[2] = v.re;
-            dst[3] = v.im;
-            u_prod = u_prod * c64{rot.x, rot.y};
+            const double* rg = ts->rg[lane];
+            const c64 rot = c64{rg[0], rg[1]}, gap = c64{rg[2], rg[3]}, g = c64{rg[4], rg[5]};
+            c64 uu = u_prod, vv = u_prod * gap;
+#pragma unroll
+            for (int i = 0; i < NI; i++) {
+                double* dst = ts->uv[j & 1][lane][i];
+                dst[0] = uu.re;
+                dst[1] = uu.im;
+                dst[2] = vv.re;
+                dst[3] = vv.im;
+                if (i + 1 < NI) {
+                    uu = uu * g;
+                    vv = vv * g;
+                }
+            }
+            u_prod = u_prod * rot;
         }
         __syncwarp();
         // field samples at the two Gauss points of every interval (FP64)
@@ -496,11 +501,11 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
 #pragma unroll
             for (int k = 0; k < kBulkTones; k++) {
                 const int slot = c * kBulkTones + k;
-                const double2 uu = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][0]);
-                const double2 vv = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][2]);
+                const double2 lv = *reinterpret_cast<const double2*>(ts->l[slot][lane]);
 #pragma unroll
                 for (int i = 0; i < NI; i++) {
-                    const double2 lv = *reinterpret_cast<const double2*>(ts->l[slot][i][lane]);
+                    const double2 uu = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][i][0]);
+                    const double2 vv = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][i][2]);
                     if (k & 1) {
                         pa[i] = fma(lv.x, uu.y, fma(lv.y, uu.x, pa[i]));
                         pb[i] = fma(lv.x, vv.y, fma(lv.y, vv.x, pb[i]));
