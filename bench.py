@@ -107,7 +107,7 @@ def algorithmic_flops(specs, form):
 
 # ------------------------------------------------------------------------------------ helpers
 class ClockSampler:
-    """SM clock and throttle reasons sampled through NVML every 10 ms during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every 2 ms during the timed region."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
                "sw_power_cap": 0x4}
@@ -136,7 +136,7 @@ class ClockSampler:
                                 self.reasons.add(name)
                     except Exception:
                         pass
-                    self._stop.wait(0.01)
+                    self._stop.wait(0.002)
 
             self.thread = threading.Thread(target=run, daemon=True)
             self.thread.start()
@@ -259,6 +259,7 @@ def bench_ours(args, world, rank):
                 batch.replay()
             e.record(stream)
             times.append((s, e))
+            e.synchronize()  # host waits here (GIL released), so the clock sampler runs during the step
         torch.cuda.synchronize()
         return [s.elapsed_time(e) / 1e3 for s, e in times]
 
@@ -432,8 +433,6 @@ def bench_serving(args):
     rates = [float(r) for r in args.rates.split(",")]
     out = {"metric": "serving p50/p99 latency and steps/s", "workload": "serving", "requests_per_rate": args.requests,
            "precision": "fp32_bulk", "hbm_budget_gb": args.hbm_budget_gb, "rates": {}}
-    warm = synthetic_requests(64, 1e5, seed=99, max_duration=1e-3)
-    Server(precision=ss.Precision.FP32_BULK).run(warm)
     for rate in rates:
         reqs = synthetic_requests(args.requests, rate, seed=4)
         srv = Server(precision=ss.Precision.FP32_BULK, hbm_budget=int(args.hbm_budget_gb * (1 << 30)),
@@ -442,7 +441,10 @@ def bench_serving(args):
         done = srv.run(reqs)
         torch.cuda.synchronize()
         summ = latency_summary(done)
-        summ.update({"launches": srv.stats["launches"], "budget_waits": srv.stats["budget_waits"]})
+        dur = [c - a for _, _, a, c in srv.launch_log]
+        summ.update({"launches": srv.stats["launches"], "budget_waits": srv.stats["budget_waits"],
+                     "launch_ms_p50": 1e3 * float(np.percentile(dur, 50)), "launch_ms_max": 1e3 * float(max(dur)),
+                     "requests_per_launch_mean": float(np.mean([n for n, _, _, _ in srv.launch_log]))})
         out["rates"][str(int(rate))] = summ
         print(json.dumps({"rate": rate, **summ}), file=sys.stderr, flush=True)
     return out

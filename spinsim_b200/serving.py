@@ -48,6 +48,12 @@ class Request:
         return Instance(self.spin, self.time_start, self.time_end, self.time_step_integration,
                         self.time_step_output, self.state_init, field=self.field)
 
+    def steps(self):
+        """Integration steps of the request (N output steps x K fine steps)."""
+        n = max(0, int((float(self.time_end) - float(self.time_start)) / float(self.time_step_output)))
+        k = int(math.floor(float(self.time_step_output) / float(self.time_step_integration) + 0.5))
+        return n * max(k, 1)
+
     def footprint(self):
         """Device bytes of the request's outputs (time, U, state, spin) and scan scratch."""
         d = self.spin.dimension
@@ -69,10 +75,13 @@ class Completed:
 
 class Server:
     """Continuous-batching evaluator.  ``hbm_budget`` bytes of outputs and scratch may be in flight
-    on up to ``streams`` concurrent launches of at most ``max_batch`` requests each."""
+    on up to ``streams`` concurrent launches of at most ``max_batch`` requests and
+    ``max_steps_per_launch`` integration steps each (a longer request runs alone), which bounds how
+    long one launch holds the requests admitted with it."""
 
     def __init__(self, precision=Precision.FP32_BULK, hbm_budget=8 << 30, streams=4, max_batch=4096,
-                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=128):
+                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=128,
+                 max_steps_per_launch=400_000_000, warm_up=True):
         import torch
         self.precision = Precision(precision)
         self.hbm_budget = int(hbm_budget)
@@ -82,8 +91,15 @@ class Server:
         self.kw = dict(precision=self.precision, number_of_squares=number_of_squares, lanes=1,
                        threads_per_block=threads_per_block, max_registers=max_registers,
                        exponentiation_half=ExponentiationMethod.ANALYTIC, force_mixed=True)
+        self.max_steps = int(max_steps_per_launch)
         self.plans = {}
         self.stats = collections.Counter()
+        self.launch_log = []  # (requests, steps, admitted at, completed at)
+        if warm_up:  # create the plan and load the kernels before the first request arrives
+            probe = Request(SpinQuantumNumber.HALF, TabulatedField({0: ([0.0, 1e-6], [0.0, 0.0])}, order=0),
+                            0.0, 2e-6, 1e-7, 1e-6, SpinQuantumNumber.HALF.plus_z)
+            b, ev = self._launch([probe], self.streams[0])
+            ev.synchronize()
 
     def _launch(self, reqs, stream):
         import torch
@@ -124,18 +140,23 @@ class Server:
                     used -= nbytes
                     free_streams.append(si)
                     self.stats["launches"] += 1
+                    self.launch_log.append((len(reqs), b.total_steps, adm, tdone))
                 else:
                     still.append(item)
             inflight = still
             # admission: one launch per free stream from the head of the queue
             while queue and free_streams:
-                take, nbytes = [], 0
+                take, nbytes, steps = [], 0, 0
                 while queue and len(take) < self.max_batch:
                     fp = queue[0].footprint()
+                    st = queue[0].steps()
                     if used + nbytes + fp > self.hbm_budget:
+                        break
+                    if take and steps + st > self.max_steps:
                         break
                     take.append(queue.popleft())
                     nbytes += fp
+                    steps += st
                 if not take:
                     self.stats["budget_waits"] += 1
                     break
