@@ -181,6 +181,14 @@ int spinsim_spin(int32_t dim, const double* state_dev, int64_t n_out, double* sp
  * the descriptors and the longest-first tile queue into the workspace (stream-ordered) and returns a
  * handle; launch issues only kernel launches and a counter reset, so it can be captured into a CUDA
  * graph and replayed.  Outputs are the flat arrays addressed by the instances' offsets. */
+/* Batch descriptors from evaluate() arguments (host only): for each instance i the step
+ * normalisation of I:1025-1034 (as spinsim_normalise_steps), its output offsets packed one after
+ * another in the flat arrays, field index i and psi0 from psi0[6 i .. 6 i + 2 dim) (re, im
+ * interleaved).  totals (optional) receives {output steps, U doubles, state doubles, integration
+ * steps}.  The batched counterpart of the per-call set-up in evaluate (I:1025-1052). */
+int spinsim_batch_describe(int32_t n, const double* t0, const double* t1, const double* dt_int, const double* dt_out,
+                           const int32_t* dim, const double* psi0, spinsim_instance* out, int64_t* totals);
+
 size_t spinsim_batch_workspace_size(const spinsim_plan* plan, const spinsim_instance* instances,
                                     int32_t n_instances, int32_t n_fields);
 int spinsim_batch_prepare(const spinsim_plan* plan, const spinsim_instance* instances, int32_t n_instances,

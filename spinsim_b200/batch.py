@@ -44,13 +44,20 @@ class Batch:
     ``exponentiation_one`` (defaults: analytic for spin half, Lie-Trotter for spin one, I:529-533),
     ``use_rotating_frame``, ``number_of_squares``, ``precision``, ``lanes``, ``threads_per_block``,
     ``max_registers`` (the last three are picked by ``spinsim_b200.autotune.tune``), ``force_mixed``
-    (use the mixed-spin kernel even for a single-spin batch).
+    (use the mixed-spin kernel even for a single-spin batch), ``memory`` (a callable taking a byte
+    count and returning a 256-byte aligned uint8 CUDA tensor of at least that size; default
+    ``torch.empty``).  All device buffers of the batch (outputs, workspace, fields, sweep
+    parameters) are carved from that one allocation, ``device_bytes`` long; the uploads run on the
+    current stream.  ``staging`` (optional): a pinned float64 host tensor the field arrays are
+    packed into for an asynchronous upload; the caller must not reuse it before that upload has
+    completed on the current stream.
     """
 
     def __init__(self, instances, get_field=None, integration_method=IntegrationMethod.MAGNUS_CF4,
                  exponentiation_half=ExponentiationMethod.ANALYTIC, exponentiation_one=ExponentiationMethod.LIE_TROTTER,
                  use_rotating_frame=True, number_of_squares=24, precision=Precision.FP64, lanes=0,
-                 threads_per_block=0, max_registers=0, plan_cache=None, force_mixed=False):
+                 threads_per_block=0, max_registers=0, plan_cache=None, force_mixed=False, memory=None,
+                 staging=None):
         import torch
         self.instances = list(instances)
         if not self.instances:
@@ -98,79 +105,93 @@ class Batch:
             if plan_cache is not None:
                 plan_cache[key] = plan
 
-        # Descriptors and output layout.
+        # Descriptors and output layout (step normalisation and offsets in the library).
         n = len(self.instances)
         insts = (_lib.Instance * n)()
-        fields = []
+        psi0 = np.zeros((n, 6))
+        dims = np.empty(n, np.int32)
+        for k, inst in enumerate(self.instances):
+            d = dims[k] = inst.spin.dimension
+            p = np.asarray(inst.state_init, np.complex128).reshape(-1)
+            if p.size != d:
+                raise ValueError(f"instance {k}: state_init must have {d} entries")
+            psi0[k, 0:2 * d:2] = p.real
+            psi0[k, 1:2 * d:2] = p.imag
+        t0 = np.fromiter((float(i.time_start) for i in self.instances), np.float64, n)
+        t1 = np.fromiter((float(i.time_end) for i in self.instances), np.float64, n)
+        dti = np.fromiter((float(i.time_step_integration) for i in self.instances), np.float64, n)
+        dto = np.fromiter((float(i.time_step_output) for i in self.instances), np.float64, n)
+        totals = (ctypes.c_int64 * 4)()
+        _lib.check(lib.spinsim_batch_describe(n, t0.ctypes.data, t1.ctypes.data, dti.ctypes.data, dto.ctypes.data,
+                                              dims.ctypes.data, psi0.ctypes.data, insts, totals))
+        out_off, u_off, st_off, self.total_steps = (int(v) for v in totals)
+        self._inst_np = np.frombuffer(insts, dtype=np.dtype(_lib.Instance))
         keep = []
         params_host = []
-        self.layout = []
-        out_off = u_off = st_off = 0
-        self.total_steps = 0
-        for k, inst in enumerate(self.instances):
-            d = inst.spin.dimension
-            dt_int, n_out, n_fine, _ = _lib.normalise_steps(inst.time_start, inst.time_end,
-                                                            inst.time_step_integration, inst.time_step_output)
-            s = insts[k]
-            s.t0 = float(inst.time_start)
-            s.dt_int = dt_int
-            s.dt_out = float(inst.time_step_output)
-            s.n_out = n_out
-            s.n_fine = n_fine
-            s.dim = d
-            s.out_offset = out_off
-            s.u_offset = u_off
-            s.state_offset = st_off
-            s.field = k
-            psi0 = np.asarray(inst.state_init, np.complex128).reshape(-1)
-            if psi0.size != d:
-                raise ValueError(f"instance {k}: state_init must have {d} entries")
-            for j in range(d):
-                s.psi0[2 * j] = psi0[j].real
-                s.psi0[2 * j + 1] = psi0[j].imag
-            self.layout.append((out_off, u_off, st_off, n_out, d))
-            out_off += n_out
-            u_off += 2 * d * d * n_out
-            st_off += 2 * d * n_out
-            self.total_steps += n_out * n_fine
-            if get_field is not None:
-                params_host.append(np.asarray(inst.sweep_parameters, np.float64).reshape(-1))
-        self.h2d_bytes = 0
-        if get_field is None:
-            from .fields import pack_fields
-            fields, kp, nbytes = pack_fields([i.field for i in self.instances], dev)
-            keep += kp
-            self.h2d_bytes += nbytes
         if get_field is not None:
-            sizes = [max(1, p.size) for p in params_host]
-            flat = np.zeros(sum(sizes))
-            offs = np.cumsum([0] + sizes[:-1])
-            for p, o in zip(params_host, offs):
-                flat[o:o + p.size] = p
-            params_dev = torch.from_numpy(flat).to(dev)
-            keep.append(params_dev)
-            self.h2d_bytes += flat.nbytes
-            for p, o in zip(params_host, offs):
-                f = _lib.Field()
-                f.params = params_dev.data_ptr() + 8 * int(o)
-                f.n_params = p.size
-                fields.append(f)
+            params_host = [np.asarray(i.sweep_parameters, np.float64).reshape(-1) for i in self.instances]
         self.n_intervals = out_off
-        fields_arr = (_lib.Field * n)(*fields)
-        self.h2d_bytes += ctypes.sizeof(insts) + ctypes.sizeof(fields_arr)
-        self._insts, self._fields, self._keep = insts, fields_arr, keep
-        self.time = torch.empty(max(1, out_off), dtype=torch.float64, device=dev)
-        self.u = torch.empty(max(1, u_off // 2), dtype=torch.complex128, device=dev)
-        self.state = torch.empty(max(1, st_off // 2), dtype=torch.complex128, device=dev)
-        self.spin = torch.empty((max(1, out_off), 3), dtype=torch.float64, device=dev)
         ws_bytes = lib.spinsim_batch_workspace_size(self._plan, insts, n, n)
         if ws_bytes == 0:
             raise ValueError(_lib.last_error() or "batch layout rejected")
-        self.workspace = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+        if get_field is None:
+            from .fields import packed_doubles
+            field_list = [i.field for i in self.instances]
+            field_doubles = max(4, packed_doubles(field_list))
+        else:
+            sizes = [max(1, p.size) for p in params_host]
+            offs = np.cumsum([0] + sizes[:-1]).astype(np.int64)
+            field_doubles = sum(sizes)
+        # one device allocation, 256-byte aligned pieces
+        pieces = {"time": 8 * max(1, out_off), "u": 8 * max(2, u_off), "state": 8 * max(2, st_off),
+                  "spin": 24 * max(1, out_off), "workspace": ws_bytes, "fields": 8 * field_doubles}
+        offsets, total = {}, 0
+        for name, nbytes in pieces.items():
+            offsets[name] = total
+            total += (nbytes + 255) // 256 * 256
+        self.device_bytes = total
+        if memory is None:
+            buf = torch.empty(total, dtype=torch.uint8, device=dev)
+        else:
+            buf = memory(total)
+            if buf.dtype != torch.uint8 or buf.numel() < total or buf.data_ptr() % 256:
+                raise ValueError("memory() must return a 256-byte aligned uint8 tensor of the requested size")
+        self.memory = buf
+
+        def piece(name, dtype):
+            o = offsets[name]
+            return buf[o:o + pieces[name]].view(dtype)
+
+        self.time = piece("time", torch.float64)
+        self.u = piece("u", torch.complex128)
+        self.state = piece("state", torch.complex128)
+        self.spin = piece("spin", torch.float64).view(-1, 3)
+        self.workspace = piece("workspace", torch.uint8)
+        field_dev = piece("fields", torch.float64)
+        # the field arrays go through host memory: the caller's pinned staging buffer when it is
+        # large enough (an asynchronous copy), else a pageable array (the copy waits for the stream)
+        if staging is not None and staging.numel() >= field_doubles:
+            host_t = staging[:field_doubles]
+        else:
+            host_t = torch.from_numpy(np.zeros(field_doubles))
+        host = host_t.numpy()
+        if get_field is None:
+            from .fields import pack_fields_into
+            fields_arr = pack_fields_into(field_list, host, field_dev.data_ptr())
+        else:
+            from .fields import FIELD_DTYPE
+            for p, o in zip(params_host, offs):
+                host[o:o + p.size] = p
+            fields_arr = np.zeros(n, FIELD_DTYPE)
+            fields_arr["params"] = field_dev.data_ptr() + 8 * offs
+            fields_arr["n_params"] = [p.size for p in params_host]
+        field_dev.copy_(host_t, non_blocking=host_t.is_pinned())
+        self.h2d_bytes = 8 * field_doubles + ctypes.sizeof(insts) + fields_arr.nbytes
+        self._insts, self._fields, self._keep = insts, fields_arr, keep
         handle = ctypes.c_void_p()
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.spinsim_batch_prepare(self._plan, insts, n, fields_arr, n, self.workspace.data_ptr(), ws_bytes,
-                                             stream, ctypes.byref(handle)))
+        _lib.check(lib.spinsim_batch_prepare(self._plan, insts, n, fields_arr.ctypes.data, n, self.workspace.data_ptr(),
+                                             ws_bytes, stream, ctypes.byref(handle)))
         self._handle = handle
         self._graph = None
 
@@ -207,20 +228,30 @@ class Batch:
         _lib.check(self.lib.spinsim_plan_get_info(self._plan, ctypes.byref(info)))
         return {k: getattr(info, k) for k, _ in _lib.PlanInfo._fields_}
 
-    def result(self, k):
-        """Results of instance k (views of the batch's device arrays)."""
-        out_off, u_off, st_off, n_out, d = self.layout[k]
+    def layout_of(self, k):
+        """(output offset, U offset, state offset (in doubles), N, d) of instance k."""
+        r = self._inst_np[k]
+        return int(r["out_offset"]), int(r["u_offset"]), int(r["state_offset"]), int(r["n_out"]), int(r["dim"])
+
+    @property
+    def layout(self):
+        return [self.layout_of(k) for k in range(len(self.instances))]
+
+    def result(self, k, keep=None):
+        """Results of instance k (views of the batch's device arrays; ``keep`` is held by the
+        Results for as long as it lives)."""
+        out_off, u_off, st_off, n_out, d = self.layout_of(k)
         time = self.time[out_off:out_off + n_out]
         u = self.u[u_off // 2:u_off // 2 + n_out * d * d].view(n_out, d, d)
         st = self.state[st_off // 2:st_off // 2 + n_out * d].view(n_out, d)
         sp = self.spin[out_off:out_off + n_out]
-        return Results(time, u, st, None, spin=sp)
+        return Results(time, u, st, None, spin=sp, keep=keep)
 
     def final_states(self):
         """state[N-1] of every instance as a list of numpy arrays."""
         st = self.state.cpu().numpy()
         out = []
-        for out_off, u_off, st_off, n_out, d in self.layout:
+        for out_off, u_off, st_off, n_out, d in map(self.layout_of, range(len(self.instances))):
             out.append(st[st_off // 2 + (n_out - 1) * d: st_off // 2 + n_out * d] if n_out else np.zeros(d, complex))
         return out
 

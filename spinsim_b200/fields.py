@@ -54,6 +54,7 @@ class TabulatedField(BuiltinField):
             raise NotImplementedError(
                 f"Interpolation order {order} is not implemented. Try order 0 (zero order hold), 1 (linear) or 3 (cubic).")
         self.tables = {}
+        snapshots = {}  # channels given the same time array share one copy (packed once)
         for c, spec in dict(channels).items():
             idx = _channel_index(c)
             t, a = np.asarray(spec[0], np.float64), np.asarray(spec[1], np.float64)
@@ -66,7 +67,9 @@ class TabulatedField(BuiltinField):
                 raise ValueError("a table needs matching time and amplitude arrays of at least two samples")
             if o not in (0, 1, 3):
                 raise NotImplementedError(f"Interpolation order {o} is not implemented.")
-            self.tables[idx] = (np.ascontiguousarray(t), np.ascontiguousarray(a), o, zb)
+            if id(spec[0]) not in snapshots:
+                snapshots[id(spec[0])] = (spec[0], t.copy())  # (the input, kept alive so its id stays unique)
+            self.tables[idx] = (snapshots[id(spec[0])][1], a.copy(), o, zb)
         self.bias = np.zeros(8)
         self.gain = np.ones(8)
         if bias is not None:
@@ -158,64 +161,107 @@ class ToneField(BuiltinField):
         return out
 
 
+_TABLE_DOUBLES = 4  # one spinsim_table is 32 bytes
+FIELD_DTYPE = np.dtype(_lib.Field)
+TABLE_DTYPE = np.dtype(_lib.Table)
+
+
+def _check_fields(fields):
+    if not all(isinstance(f, (TabulatedField, ToneField)) for f in fields) or len({f.kind for f in fields}) > 1:
+        raise TypeError("packed fields must be built-in fields of one kind")
+
+
+def packed_doubles(fields):
+    """float64 entries the fields take in a packed field buffer (``pack_fields_into``): per table
+    its times and amplitudes, each padded to 32 bytes, and eight 32-byte table descriptors per
+    tabulated field; the (w, A, phi) rows of a tone field padded to 32 bytes."""
+    _check_fields(fields)
+    total = 0
+    for f in fields:
+        if isinstance(f, TabulatedField):
+            times = {id(t): t.size for t, _, _, _ in f.tables.values()}
+            total += sum((m + 3) // 4 * 4 for m in times.values())
+            total += sum((a.size + 3) // 4 * 4 for _, a, _, _ in f.tables.values()) + 8 * _TABLE_DOUBLES
+        else:
+            total += (3 * sum(a.shape[0] for a in f.tones.values()) + 3) // 4 * 4 or 4
+    return total
+
+
+def pack_fields_into(fields, host, base):
+    """Write the fields' arrays (and table descriptors) into ``host`` (a float64 array of at least
+    ``packed_doubles(fields)`` entries) for a device copy of ``host`` at address ``base`` (32-byte
+    aligned); returns the ``spinsim_field`` structs as a numpy array of ``FIELD_DTYPE``.  Padding
+    entries are left as they are."""
+    _check_fields(fields)
+    n = len(fields)
+    out = np.zeros(n, FIELD_DTYPE)
+    if not n:
+        return out
+    at = 0
+    if isinstance(fields[0], TabulatedField):
+        slot, t_at, a_at, size, order, zb, desc = [], [], [], [], [], [], []
+        for f in fields:
+            first = len(slot)
+            written = {}
+            for c, (t, a, o, z) in f.tables.items():
+                m = t.size
+                p = (m + 3) // 4 * 4
+                ti = written.get(id(t))
+                if ti is None:
+                    host[at:at + m] = t
+                    ti = written[id(t)] = at
+                    at += p
+                host[at:at + m] = a
+                slot.append(c)
+                t_at.append(ti)
+                a_at.append(at)
+                size.append(m)
+                order.append(o)
+                zb.append(z)
+                at += p
+            host[at:at + 8 * _TABLE_DOUBLES] = 0.0
+            desc.append(at)
+            for k in range(first, len(slot)):
+                slot[k] += at // _TABLE_DOUBLES
+            at += 8 * _TABLE_DOUBLES
+        tab = host[:at].view(TABLE_DTYPE)
+        slot = np.array(slot, np.int64)
+        tab["time"][slot] = base + 8 * np.array(t_at, np.uint64)
+        tab["amplitude"][slot] = base + 8 * np.array(a_at, np.uint64)
+        tab["size"][slot] = size
+        tab["order"][slot] = order
+        tab["zero_boundary"][slot] = zb
+        out["tables"] = base + 8 * np.array(desc, np.uint64)
+        out["bias"] = np.stack([f.bias for f in fields])
+        out["gain"] = np.stack([f.gain for f in fields])
+    else:
+        starts = []
+        for k, f in enumerate(fields):
+            flat, start, count = f.packed()
+            host[at:at + flat.size] = flat
+            starts.append(at)
+            out["tone_start"][k] = start
+            out["tone_count"][k] = count
+            at += (flat.size + 3) // 4 * 4 or 4
+        out["tones"] = base + 8 * np.array(starts, np.uint64)
+        out["bias"] = np.stack([f.bias for f in fields])
+        out["gain"] = 1.0
+    return out
+
+
 def pack_fields(fields, device):
     """Device structs for a list of built-in fields with one host-to-device copy.
 
     All tone arrays, table arrays and table descriptors go into one float64 buffer; returns
-    (list of ctypes Field, [device buffer], host bytes copied)."""
-    import ctypes
+    (numpy array of spinsim_field structs, [device buffer], host bytes copied)."""
     import torch
-    chunks = []
-    n = 0
-
-    def put(arr):
-        nonlocal n
-        arr = np.ascontiguousarray(arr, np.float64).reshape(-1)
-        off = n
-        chunks.append(arr)
-        n += arr.size
-        pad = (-n) % 4  # keep every chunk 32-byte aligned
-        if pad:
-            chunks.append(np.zeros(pad))
-            n += pad
-        return off
-
-    plan = []
-    for f in fields:
-        if isinstance(f, ToneField):
-            flat, start, count = f.packed()
-            plan.append(("tones", f, put(flat), start, count))
-        elif isinstance(f, TabulatedField):
-            offs = {idx: (put(t), put(a), t.size, o, zb) for idx, (t, a, o, zb) in f.tables.items()}
-            tab_off = put(np.zeros(8 * ctypes.sizeof(_lib.Table) // 8))
-            plan.append(("table", f, tab_off, offs, None))
-        else:
-            raise TypeError("not a built-in field")
-    host = np.concatenate(chunks) if chunks else np.zeros(4)
-    dev = torch.empty(host.size, dtype=torch.float64, device=device)
-    base = dev.data_ptr()
-    out = []
-    for kind, f, off, a, b in plan:
-        st = _lib.Field()
-        if kind == "tones":
-            st.tones = base + 8 * off
-            for c in range(8):
-                st.tone_start[c] = int(a[c])
-                st.tone_count[c] = int(b[c])
-                st.bias[c] = f.bias[c]
-                st.gain[c] = 1.0
-        else:
-            tabs = (_lib.Table * 8)()
-            for idx, (to, ao, size, o, zb) in a.items():
-                tabs[idx] = _lib.Table(base + 8 * to, base + 8 * ao, size, o, int(zb))
-            host[off:off + 8 * ctypes.sizeof(_lib.Table) // 8] = np.frombuffer(bytes(tabs), np.float64)
-            st.tables = base + 8 * off
-            for c in range(8):
-                st.bias[c] = f.bias[c]
-                st.gain[c] = f.gain[c]
-        out.append(st)
+    fields = list(fields)
+    total = max(4, packed_doubles(fields))
+    dev = torch.empty(total, dtype=torch.float64, device=device)
+    host = np.zeros(total)
+    structs = pack_fields_into(fields, host, dev.data_ptr())
     dev.copy_(torch.from_numpy(host))
-    return out, [dev], host.nbytes
+    return structs, [dev], host.nbytes
 
 
 # ---------------------------------------------------------------------------- sampler factory

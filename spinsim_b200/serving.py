@@ -3,23 +3,31 @@
 Requests (one ``evaluate`` each: spin, field, time span, steps, initial state) arrive over time.
 The server keeps a queue and a set of in-flight launches on several CUDA streams:
 
-* **admission** — a request is admitted when a stream slot is free and its device footprint
-  (outputs + scan workspace, counted from the sizes the C ABI reports) fits the HBM budget;
+* **device memory** — the server takes ``hbm_budget`` bytes of HBM once, at start-up, as one
+  arena; every launch carves its outputs, workspace and field tables from it (first fit, 256-byte
+  aligned), so the serving loop never calls the CUDA allocator (whose cudaMalloc stalls the host
+  for tens of milliseconds);
+* **admission** — a request is admitted when a stream slot is free and its device footprint (an
+  upper bound on the bytes of its outputs, scratch and field) fits the arena's largest free block;
 * **continuous batching** — all requests admitted together form one persistent launch (the
   ``Batch`` path: one time-evolution launch over a longest-first tile queue, then the segmented
   state scan); requests that arrive while earlier launches run form the next launch on another
   stream, so their work overlaps on the device;
 * **completion** — each launch records an event; when it has passed, the launch's requests are
-  resolved with their ``Results`` (device tensors; numpy on access, or copied to the host when
-  ``copy_to_host``), and their memory returns to the budget.
+  resolved with their ``Results`` (views of the arena; numpy on access, or copied to the host when
+  ``copy_to_host``).  A launch's block returns to the arena when its last ``Results`` is released,
+  so results the caller keeps hold budget, and results it drops free it.
 
 Every request runs in the same kernel (the mixed-spin plan, one lane per output step, fixed scan
 tiles), so its result does not depend on what else is in the launch: alone and in the mix agree
 bit for bit.  Latency is measured on the host clock from arrival to completion.
 """
+import bisect
 import collections
+import gc
 import math
 import time
+import weakref
 from dataclasses import dataclass, field as dc_field
 from typing import Any, Optional
 
@@ -55,11 +63,22 @@ class Request:
         return n * max(k, 1)
 
     def footprint(self):
-        """Device bytes of the request's outputs (time, U, state, spin) and scan scratch."""
+        """Upper bound on the device bytes the request takes in a launch, even alone in it.
+
+        Outputs (time 8, U 16 d^2, state 16 d, spin 24 bytes per output step); the launch workspace
+        (a 120-byte instance and 224-byte field descriptor, time-evolution tiles of 16 bytes per 32
+        steps at most, and per scan tile of 2,048 steps a 16-byte tile, 256 thread prefixes and two
+        tile products of 16 d^2 bytes each); the field (tables or tones, 32-byte aligned chunks, and
+        eight 32-byte table descriptors); 256-byte alignment of every piece."""
         d = self.spin.dimension
         n = max(0, int((float(self.time_end) - float(self.time_start)) / float(self.time_step_output)))
-        return n * (8 + 16 * d * d + 16 * d + 24) + n * 16 * d * d // 8 + 4096
-
+        fld = 256
+        tables = getattr(self.field, "tables", None)
+        if tables is not None:
+            fld += sum(16 * t.size + 48 for t, _, _, _ in tables.values())
+        elif self.field is not None and hasattr(self.field, "packed"):
+            fld += 8 * self.field.packed()[0].size + 24
+        return n * (33 + 16 * d + 19 * d * d) + 4160 * d * d + 6400 + fld
 
 @dataclass
 class Completed:
@@ -73,19 +92,83 @@ class Completed:
         return self.completed - self.request.arrival
 
 
+class Arena:
+    """One device allocation handed out in 256-byte aligned blocks (first fit, coalescing frees)."""
+
+    ALIGN = 256
+
+    def __init__(self, nbytes, device="cuda"):
+        import torch
+        self.size = (int(nbytes) + self.ALIGN - 1) // self.ALIGN * self.ALIGN
+        self.buffer = torch.empty(self.size, dtype=torch.uint8, device=device)
+        self._starts = [0]          # free blocks, sorted by offset
+        self._sizes = {0: self.size}
+        self.in_use = 0
+
+    def largest_free(self):
+        return max(self._sizes.values(), default=0)
+
+    def take(self, nbytes):
+        """Offset of a free block of ``nbytes`` (rounded up to the alignment), or None."""
+        n = (int(nbytes) + self.ALIGN - 1) // self.ALIGN * self.ALIGN
+        for i, off in enumerate(self._starts):
+            size = self._sizes[off]
+            if size >= n:
+                del self._sizes[off]
+                if size == n:
+                    del self._starts[i]
+                else:
+                    self._starts[i] = off + n
+                    self._sizes[off + n] = size - n
+                self.in_use += n
+                return off, n
+        return None
+
+    def give(self, off, n):
+        """Return the block [off, off + n) (from ``take``)."""
+        self.in_use -= n
+        i = bisect.bisect_left(self._starts, off)
+        if i < len(self._starts) and off + n == self._starts[i]:  # merge with the next block
+            nxt = self._starts.pop(i)
+            n += self._sizes.pop(nxt)
+        if i > 0 and self._starts[i - 1] + self._sizes[self._starts[i - 1]] == off:  # with the previous
+            self._sizes[self._starts[i - 1]] += n
+        else:
+            self._starts.insert(i, off)
+            self._sizes[off] = n
+
+
+class _Lease:
+    """Holds one launch's arena block; the block returns to the arena when the lease is released
+    (when the launch's Batch and every Results made from it are gone)."""
+
+    def __init__(self, arena, off, n):
+        self.block = (off, n)
+        weakref.finalize(self, arena.give, off, n)
+
+
+class ArenaFull(Exception):
+    pass
+
+
 class Server:
-    """Continuous-batching evaluator.  ``hbm_budget`` bytes of outputs and scratch may be in flight
-    on up to ``streams`` concurrent launches of at most ``max_batch`` requests and
+    """Continuous-batching evaluator.  ``hbm_budget`` bytes of HBM (one arena, taken at start-up)
+    hold the outputs and scratch of launches in flight and of results the caller still holds; up to
+    ``streams`` launches run concurrently, of at most ``max_batch`` requests and
     ``max_steps_per_launch`` integration steps each (a longer request runs alone), which bounds how
     long one launch holds the requests admitted with it."""
 
     def __init__(self, precision=Precision.FP32_BULK, hbm_budget=8 << 30, streams=4, max_batch=4096,
                  copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=128,
-                 max_steps_per_launch=400_000_000, warm_up=True):
+                 max_steps_per_launch=400_000_000, warm_up=True, staging_bytes=32 << 20):
         import torch
         self.precision = Precision(precision)
         self.hbm_budget = int(hbm_budget)
+        self.arena = Arena(self.hbm_budget)
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
+        # pinned host staging for each stream's field upload (reused once the stream's launch is done)
+        self.staging = [torch.empty(int(staging_bytes) // 8, dtype=torch.float64, pin_memory=True)
+                        for _ in range(streams)]
         self.max_batch = max_batch
         self.copy_to_host = copy_to_host
         self.kw = dict(precision=self.precision, number_of_squares=number_of_squares, lanes=1,
@@ -95,76 +178,71 @@ class Server:
         self.plans = {}
         self.stats = collections.Counter()
         self.launch_log = []  # (requests, steps, admitted at, completed at)
-        if warm_up:  # create the plan and load the kernels before the first request arrives
+        if warm_up:
+            # create the plan and load the kernels before the first request arrives
             probe = Request(SpinQuantumNumber.HALF, TabulatedField({0: ([0.0, 1e-6], [0.0, 0.0])}, order=0),
                             0.0, 2e-6, 1e-7, 1e-6, SpinQuantumNumber.HALF.plus_z)
-            b, ev = self._launch([probe], self.streams[0])
-            ev.synchronize()
+            with torch.cuda.stream(self.streams[0]):
+                Batch([probe.instance()], plan_cache=self.plans, **self.kw).run()
+            self.streams[0].synchronize()
 
-    def _launch(self, reqs, stream):
+    def _launch(self, reqs, si):
+        """Place a launch in the arena, upload its descriptors and run it on ``stream`` (free, so the
+        uploads' stream synchronisation does not wait on other work).  Raises ArenaFull when the
+        launch does not fit."""
         import torch
+        lease = []
+
+        def memory(nbytes):
+            blk = self.arena.take(nbytes)
+            if blk is None:
+                raise ArenaFull(nbytes)
+            lease.append(_Lease(self.arena, *blk))
+            return self.arena.buffer[blk[0]:blk[0] + blk[1]]
+
+        stream = self.streams[si]
         with torch.cuda.stream(stream):
-            b = Batch([r.instance() for r in reqs], plan_cache=self.plans, **self.kw)
+            b = Batch([r.instance() for r in reqs], plan_cache=self.plans, memory=memory, staging=self.staging[si],
+                      **self.kw)
+            b.lease = lease[0]
             b.run()
+            ev = torch.cuda.Event()
             if self.copy_to_host:
                 b.host = [t.to("cpu", non_blocking=True) for t in (b.time, b.u, b.state, b.spin)]
-            ev = torch.cuda.Event()
             ev.record(stream)
-        return b, ev
+        return b, ev, lease[0]
 
-    def run(self, requests, clock=time.perf_counter, idle_sleep=20e-6):
+    def run(self, requests, clock=time.perf_counter, idle_sleep=20e-6, on_complete=None, keep_results=True):
         """Serve ``requests`` (arrival times in seconds from the start) in open loop; returns the
-        list of ``Completed`` in completion order."""
+        list of ``Completed`` in completion order.  ``on_complete(completed)`` is called as each
+        request completes; with ``keep_results=False`` the returned ``Completed`` carry no results
+        (their device memory goes back to the arena once ``on_complete`` returns)."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         for r in pending:
-            if r.footprint() > self.hbm_budget:
+            if r.footprint() > self.arena.size:
                 raise ValueError(f"request {r.id} needs {r.footprint()} bytes, above the HBM budget")
+        gc_was_enabled = gc.isenabled()
+        gc.disable()  # a full collection over the live results would stall the loop for tens of ms
+        try:
+            return self._run(pending, clock, idle_sleep, on_complete, keep_results)
+        finally:
+            if gc_was_enabled:
+                gc.enable()
+
+    def _run(self, pending, clock, idle_sleep, on_complete, keep_results):
         queue = collections.deque()
-        inflight = []  # (batch, event, requests, bytes, stream index, admitted time)
+        inflight = []  # (batch, event, requests, stream index, admitted time)
         free_streams = list(range(len(self.streams)))
-        used = 0
         done = []
         t0 = clock()
         while pending or queue or inflight:
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
-            # completions
-            still = []
-            for item in inflight:
-                b, ev, reqs, nbytes, si, adm = item
-                if ev.query():
-                    tdone = clock() - t0
-                    for k, r in enumerate(reqs):
-                        done.append(Completed(r, b.result(k), adm, tdone))
-                    used -= nbytes
-                    free_streams.append(si)
-                    self.stats["launches"] += 1
-                    self.launch_log.append((len(reqs), b.total_steps, adm, tdone))
-                else:
-                    still.append(item)
-            inflight = still
-            # admission: one launch per free stream from the head of the queue
+            inflight = self._complete(inflight, free_streams, done, clock, t0, on_complete, keep_results)
             while queue and free_streams:
-                take, nbytes, steps = [], 0, 0
-                while queue and len(take) < self.max_batch:
-                    fp = queue[0].footprint()
-                    st = queue[0].steps()
-                    if used + nbytes + fp > self.hbm_budget:
-                        break
-                    if take and steps + st > self.max_steps:
-                        break
-                    take.append(queue.popleft())
-                    nbytes += fp
-                    steps += st
-                if not take:
-                    self.stats["budget_waits"] += 1
+                if not self._admit(queue, inflight, free_streams, clock, t0):
                     break
-                si = free_streams.pop()
-                b, ev = self._launch(take, self.streams[si])
-                used += nbytes
-                inflight.append((b, ev, take, nbytes, si, clock() - t0))
-                self.stats["admitted"] += len(take)
             if not (queue and free_streams) and (inflight or pending):
                 if pending and not queue and not inflight:
                     wait = pending[0].arrival - (clock() - t0)
@@ -173,6 +251,72 @@ class Server:
                 else:
                     time.sleep(idle_sleep)
         return done
+
+    def _complete(self, inflight, free_streams, done, clock, t0, on_complete, keep_results):
+        """Resolve the launches whose event has passed; returns the launches still running."""
+        still = []
+        for item in inflight:
+            b, ev, reqs, si, adm = item
+            if not ev.query():
+                still.append(item)
+                continue
+            tdone = clock() - t0
+            for k, r in enumerate(reqs):
+                c = Completed(r, b.result(k, keep=b.lease), adm, tdone)
+                if on_complete is not None:
+                    on_complete(c)
+                if not keep_results:
+                    c.results = None
+                done.append(c)
+            free_streams.append(si)
+            self.stats["launches"] += 1
+            self.launch_log.append((len(reqs), b.total_steps, adm, tdone))
+        return still
+
+    def _admit(self, queue, inflight, free_streams, clock, t0):
+        """Start one launch from the head of the queue on a free stream; False when nothing fits
+        (wait for a completion or a released result)."""
+        avail = self.arena.largest_free()
+        take, nbytes, steps = [], 0, 0
+        while queue and len(take) < self.max_batch:
+            fp = queue[0].footprint()
+            st = queue[0].steps()
+            if nbytes + fp > avail:
+                break
+            if take and steps + st > self.max_steps:
+                break
+            take.append(queue.popleft())
+            nbytes += fp
+            steps += st
+        if not take:
+            self.stats["budget_waits"] += 1
+            if not inflight:
+                gc.collect()  # results released only through a reference cycle
+                if self.arena.largest_free() < queue[0].footprint():
+                    raise RuntimeError("the HBM budget is held by results still referenced: release Results "
+                                       "(or serve with keep_results=False) or raise hbm_budget")
+                return True
+            return False
+        si = free_streams.pop()
+        while True:
+            try:
+                b, ev, _ = self._launch(take, si)
+                break
+            except ArenaFull:
+                # footprints are upper bounds, so this follows only from fragmentation: launch fewer
+                self.stats["arena_retries"] += 1
+                if len(take) == 1:
+                    free_streams.append(si)
+                    queue.appendleft(take[0])
+                    if not inflight:
+                        raise RuntimeError("a request does not fit the arena's free blocks")
+                    return False
+                half = len(take) // 2
+                queue.extendleft(reversed(take[half:]))
+                take = take[:half]
+        inflight.append((b, ev, take, si, clock() - t0))
+        self.stats["admitted"] += len(take)
+        return True
 
 
 # ---------------------------------------------------------------------------- synthetic workload

@@ -1,0 +1,68 @@
+"""Packing of built-in fields into one buffer (host side): table arrays, descriptors and tone rows
+land where the spinsim_field structs point."""
+import numpy as np
+import pytest
+
+BASE = 1 << 40  # a pretend device address of the packed buffer
+
+
+def decode(host, addr):
+    return (int(addr) - BASE) // 8
+
+
+def test_tables_and_descriptors_round_trip():
+    from spinsim_b200.fields import TABLE_DTYPE, TabulatedField, pack_fields_into, packed_doubles
+    rng = np.random.default_rng(5)
+    fields = []
+    for k in range(7):
+        chans = {}
+        for c in rng.choice(8, size=rng.integers(1, 4), replace=False):
+            m = int(rng.integers(2, 40))
+            chans[int(c)] = (np.sort(rng.uniform(0, 1, m)), rng.normal(size=m), int(rng.choice([0, 1, 3])), bool(k % 2))
+        fields.append(TabulatedField(chans, bias=rng.normal(size=8), gain=rng.normal(size=8)))
+    total = packed_doubles(fields)
+    assert total % 4 == 0
+    host = np.full(total + 8, np.nan)
+    out = pack_fields_into(fields, host, BASE)
+    tabs = host.view(TABLE_DTYPE)
+    for f, st in zip(fields, out):
+        slot0 = decode(host, st["tables"]) // 4
+        assert np.array_equal(st["bias"], f.bias) and np.array_equal(st["gain"], f.gain)
+        for c in range(8):
+            row = tabs[slot0 + c]
+            if c not in f.tables:
+                assert row["size"] == 0 and row["time"] == 0
+                continue
+            t, a, o, zb = f.tables[c]
+            assert (row["size"], row["order"], row["zero_boundary"]) == (t.size, o, int(zb))
+            ti, ai = decode(host, row["time"]), decode(host, row["amplitude"])
+            assert ti % 4 == 0 and ai % 4 == 0  # 32-byte aligned
+            assert np.array_equal(host[ti:ti + t.size], t) and np.array_equal(host[ai:ai + a.size], a)
+    assert np.isnan(host[total:]).all()  # nothing written past the packed size
+
+
+def test_tones_round_trip():
+    from spinsim_b200.fields import ToneField, pack_fields_into, packed_doubles
+    rng = np.random.default_rng(6)
+    fields = [ToneField({c: rng.normal(size=(int(rng.integers(1, 5)), 3)) for c in range(3)}, bias=[0.1, 0, 2.0])
+              for _ in range(5)]
+    host = np.zeros(packed_doubles(fields))
+    out = pack_fields_into(fields, host, BASE)
+    for f, st in zip(fields, out):
+        flat, start, count = f.packed()
+        i = decode(host, st["tones"])
+        assert i % 4 == 0
+        assert np.array_equal(host[i:i + flat.size], flat)
+        assert np.array_equal(st["tone_start"], start) and np.array_equal(st["tone_count"], count)
+        assert np.array_equal(st["bias"], f.bias) and np.all(st["gain"] == 1.0)
+
+
+def test_mixed_kinds_rejected_and_tables_snapshotted():
+    from spinsim_b200.fields import TabulatedField, ToneField, packed_doubles
+    t = np.array([0.0, 1.0])
+    a = np.array([1.0, 2.0])
+    f = TabulatedField({0: (t, a)})
+    a[0] = 99.0  # the field keeps its own copy
+    assert f.tables[0][1][0] == 1.0
+    with pytest.raises(TypeError):
+        packed_doubles([f, ToneField({0: [[1.0, 1.0, 0.0]]})])

@@ -61,8 +61,41 @@ def test_hbm_budget_admission(cuda):
     reqs = requests(n=12, rate=1e6, seed=9)
     budget = max(r.footprint() for r in reqs) + 1
     srv = Server(precision=ss.Precision.FP64, hbm_budget=budget, streams=4)
-    done = srv.run(reqs)
-    assert len(done) == len(reqs)
+    seen = []
+    done = srv.run(reqs, on_complete=lambda c: seen.append(float(c.results.state[-1, 0].real)), keep_results=False)
+    assert len(done) == len(reqs) == len(seen)
+    assert all(c.results is None for c in done)
     assert srv.stats["budget_waits"] > 0
+    assert srv.arena.in_use == 0
     with pytest.raises(ValueError):
         Server(precision=ss.Precision.FP64, hbm_budget=1000).run(reqs[:1])
+
+
+def test_held_results_hold_the_budget(cuda):
+    import gc
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Server
+    reqs = requests(n=12, rate=1e6, seed=9)
+    srv = Server(precision=ss.Precision.FP64, hbm_budget=max(r.footprint() for r in reqs) + 1, streams=2)
+    with pytest.raises(RuntimeError, match="held by results"):
+        srv.run(reqs)  # keeps every result: the arena fills up
+    gc.collect()
+    assert srv.arena.in_use == 0
+    big = Server(precision=ss.Precision.FP64, hbm_budget=256 << 20, streams=2)
+    done = big.run(reqs)
+    held = big.arena.in_use
+    assert 0 < held <= sum(r.footprint() for r in reqs)
+    del done
+    gc.collect()
+    assert big.arena.in_use == 0
+
+
+def test_footprint_bounds_the_launch(cuda):
+    import spinsim_b200 as ss
+    from spinsim_b200.batch import Batch
+    from spinsim_b200.serving import Server
+    reqs = requests(n=16, rate=1e6, seed=11, max_duration=2e-3)
+    srv = Server(precision=ss.Precision.FP32_BULK, warm_up=False)
+    for group in (reqs[:1], reqs[1:2], reqs[:8], reqs):
+        b = Batch([r.instance() for r in group], **srv.kw)
+        assert b.device_bytes <= sum(r.footprint() for r in group)
