@@ -194,6 +194,17 @@ size_t spinsim_batch_workspace_size(const spinsim_plan* plan, const spinsim_inst
 int spinsim_batch_prepare(const spinsim_plan* plan, const spinsim_instance* instances, int32_t n_instances,
                           const spinsim_field* fields, int32_t n_fields, void* workspace_dev,
                           size_t workspace_bytes, void* stream, spinsim_batch** out);
+
+/* The same preparation with every descriptor written into host_staging (at least
+ * spinsim_batch_staging_size bytes; page-locked for the copy to be asynchronous) and uploaded with
+ * one copy on `stream`; host_staging must stay unchanged until that copy has completed.  The
+ * descriptors lead the workspace, so the copy is one contiguous block. */
+size_t spinsim_batch_staging_size(const spinsim_plan* plan, const spinsim_instance* instances, int32_t n_instances,
+                                  int32_t n_fields);
+int spinsim_batch_prepare_staged(const spinsim_plan* plan, const spinsim_instance* instances, int32_t n_instances,
+                                 const spinsim_field* fields, int32_t n_fields, void* workspace_dev,
+                                 size_t workspace_bytes, void* host_staging, size_t staging_bytes, void* stream,
+                                 spinsim_batch** out);
 int spinsim_batch_launch(const spinsim_batch* batch, double* time_dev, double* u_dev, double* state_dev,
                          double* spin_dev, void* stream);
 int spinsim_batch_destroy(spinsim_batch* batch);

@@ -84,6 +84,10 @@ _SIGNATURES = [
     ("spinsim_batch_workspace_size", ctypes.c_size_t, [c_vp, ctypes.POINTER(Instance), c_i32, c_i32]),
     ("spinsim_batch_prepare", ctypes.c_int,
      [c_vp, ctypes.POINTER(Instance), c_i32, c_vp, c_i32, c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
+    ("spinsim_batch_staging_size", ctypes.c_size_t, [c_vp, ctypes.POINTER(Instance), c_i32, c_i32]),
+    ("spinsim_batch_prepare_staged", ctypes.c_int,
+     [c_vp, ctypes.POINTER(Instance), c_i32, c_vp, c_i32, c_vp, ctypes.c_size_t, c_vp, ctypes.c_size_t, c_vp,
+      ctypes.POINTER(c_vp)]),
     ("spinsim_batch_launch", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("spinsim_batch_destroy", ctypes.c_int, [c_vp]),
     ("spinsim_fma_peak", ctypes.c_int, [c_i32, ctypes.POINTER(c_dbl), c_vp]),

@@ -48,9 +48,10 @@ class Batch:
     count and returning a 256-byte aligned uint8 CUDA tensor of at least that size; default
     ``torch.empty``).  All device buffers of the batch (outputs, workspace, fields, sweep
     parameters) are carved from that one allocation, ``device_bytes`` long; the uploads run on the
-    current stream.  ``staging`` (optional): a pinned float64 host tensor the field arrays are
-    packed into for an asynchronous upload; the caller must not reuse it before that upload has
-    completed on the current stream.
+    current stream.  ``staging`` (optional): a pinned uint8 host tensor (256-byte aligned), or a
+    callable taking a byte count and returning one, that the descriptors and field arrays are
+    written into for asynchronous uploads (when it is large enough); the caller must not reuse it
+    before those uploads have completed on the current stream.
     """
 
     def __init__(self, instances, get_field=None, integration_method=IntegrationMethod.MAGNUS_CF4,
@@ -108,19 +109,27 @@ class Batch:
         # Descriptors and output layout (step normalisation and offsets in the library).
         n = len(self.instances)
         insts = (_lib.Instance * n)()
-        psi0 = np.zeros((n, 6))
-        dims = np.empty(n, np.int32)
+        rows = {}  # psi0 rows by state_init object (instances often share the basis states)
+        times, psi_rows, dim_list = [], [], []
         for k, inst in enumerate(self.instances):
-            d = dims[k] = inst.spin.dimension
-            p = np.asarray(inst.state_init, np.complex128).reshape(-1)
-            if p.size != d:
-                raise ValueError(f"instance {k}: state_init must have {d} entries")
-            psi0[k, 0:2 * d:2] = p.real
-            psi0[k, 1:2 * d:2] = p.imag
-        t0 = np.fromiter((float(i.time_start) for i in self.instances), np.float64, n)
-        t1 = np.fromiter((float(i.time_end) for i in self.instances), np.float64, n)
-        dti = np.fromiter((float(i.time_step_integration) for i in self.instances), np.float64, n)
-        dto = np.fromiter((float(i.time_step_output) for i in self.instances), np.float64, n)
+            d = inst.spin.dimension
+            key = (id(inst.state_init), d)
+            row = rows.get(key)
+            if row is None:
+                p = np.asarray(inst.state_init, np.complex128).reshape(-1)
+                if p.size != d:
+                    raise ValueError(f"instance {k}: state_init must have {d} entries")
+                row = [0.0] * 6
+                row[0:2 * d:2] = p.real.tolist()
+                row[1:2 * d:2] = p.imag.tolist()
+                rows[key] = row
+            psi_rows.append(row)
+            dim_list.append(d)
+            times.append((inst.time_start, inst.time_end, inst.time_step_integration, inst.time_step_output))
+        times = np.array(times, np.float64).reshape(n, 4).T.copy()
+        t0, t1, dti, dto = times
+        psi0 = np.array(psi_rows, np.float64)
+        dims = np.array(dim_list, np.int32)
         totals = (ctypes.c_int64 * 4)()
         _lib.check(lib.spinsim_batch_describe(n, t0.ctypes.data, t1.ctypes.data, dti.ctypes.data, dto.ctypes.data,
                                               dims.ctypes.data, psi0.ctypes.data, insts, totals))
@@ -168,10 +177,19 @@ class Batch:
         self.spin = piece("spin", torch.float64).view(-1, 3)
         self.workspace = piece("workspace", torch.uint8)
         field_dev = piece("fields", torch.float64)
-        # the field arrays go through host memory: the caller's pinned staging buffer when it is
-        # large enough (an asynchronous copy), else a pageable array (the copy waits for the stream)
-        if staging is not None and staging.numel() >= field_doubles:
-            host_t = staging[:field_doubles]
+        # Field arrays and descriptors go through host memory: the caller's pinned staging buffer
+        # when it is large enough (asynchronous copies: descriptors first, then fields), else
+        # pageable memory (the copies wait for the stream).
+        desc_bytes = 0
+        if staging is not None:
+            desc_bytes = (lib.spinsim_batch_staging_size(self._plan, insts, n, n) + 255) // 256 * 256
+            if callable(staging):
+                staging = staging(desc_bytes + 8 * field_doubles)
+            if staging.dtype != torch.uint8 or not staging.is_pinned() or \
+                    staging.numel() < desc_bytes + 8 * field_doubles or staging.data_ptr() % 256:
+                staging = None
+        if staging is not None:
+            host_t = staging[desc_bytes:desc_bytes + 8 * field_doubles].view(torch.float64)
         else:
             host_t = torch.from_numpy(np.zeros(field_doubles))
         host = host_t.numpy()
@@ -185,13 +203,21 @@ class Batch:
             fields_arr = np.zeros(n, FIELD_DTYPE)
             fields_arr["params"] = field_dev.data_ptr() + 8 * offs
             fields_arr["n_params"] = [p.size for p in params_host]
-        field_dev.copy_(host_t, non_blocking=host_t.is_pinned())
         self.h2d_bytes = 8 * field_doubles + ctypes.sizeof(insts) + fields_arr.nbytes
         self._insts, self._fields, self._keep = insts, fields_arr, keep
         handle = ctypes.c_void_p()
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.spinsim_batch_prepare(self._plan, insts, n, fields_arr.ctypes.data, n, self.workspace.data_ptr(),
-                                             ws_bytes, stream, ctypes.byref(handle)))
+        if staging is not None:
+            _lib.check(lib.spinsim_batch_prepare_staged(self._plan, insts, n, fields_arr.ctypes.data, n,
+                                                        self.workspace.data_ptr(), ws_bytes, staging.data_ptr(),
+                                                        desc_bytes, stream, ctypes.byref(handle)))
+        else:
+            _lib.check(lib.spinsim_batch_prepare(self._plan, insts, n, fields_arr.ctypes.data, n,
+                                                 self.workspace.data_ptr(), ws_bytes, stream, ctypes.byref(handle)))
+        # after the descriptor upload, so that torch's record of this copy on the pinned staging
+        # block (which keeps the block from reuse until the copy is done) covers both
+        field_dev.copy_(host_t, non_blocking=host_t.is_pinned())
+        self._staging = staging
         self._handle = handle
         self._graph = None
 
@@ -263,3 +289,110 @@ class Batch:
                 self.lib.spinsim_plan_destroy(self._plan)
         except Exception:
             pass
+
+
+class Evaluator:
+    """Evaluate lists of instances into host memory with the stages overlapped.
+
+    The list is split into ``chunks`` contiguous groups of about equal work.  Group k's host set-up
+    (descriptors, field packing into pinned staging) and kernels run while group k-1's outputs are
+    copied to pinned host memory on a second stream, so the end-to-end time approaches the larger
+    of the kernel time and the device-to-host copy time instead of their sum.  ``evaluate`` returns
+    one ``Results`` per instance whose arrays are numpy views of page-locked host buffers.
+    Remaining keyword arguments go to ``Batch``; with ``lanes`` fixed and ``force_mixed=True`` the
+    results are bit-identical to one ``Batch`` of the whole list, otherwise a group may pick other
+    lanes or a single-spin kernel and the results agree to rounding.
+    """
+
+    def __init__(self, chunks=6, **batch_kwargs):
+        import torch
+        self.chunks = max(1, int(chunks))
+        self.kw = batch_kwargs
+        self.plans = batch_kwargs.pop("plan_cache", None)
+        if self.plans is None:
+            self.plans = {}
+        self.compute = torch.cuda.Stream()
+        self.copy = torch.cuda.Stream()
+        self.h2d_bytes = self.d2h_bytes = 0
+
+    @staticmethod
+    def _pinned(nbytes):
+        import torch
+        return torch.empty(max(256, int(nbytes)), dtype=torch.uint8, pin_memory=True)
+
+    def groups(self, instances):
+        """Contiguous groups of about equal work (about (t1 - t0) / dt_int steps, spin one weighted
+        x8)."""
+        a = np.array([(i.time_start, i.time_end, i.time_step_integration, i.spin.dimension) for i in instances],
+                     np.float64).reshape(-1, 4)
+        work = np.maximum((a[:, 1] - a[:, 0]) / a[:, 2], 1.0) * np.where(a[:, 3] == 3, 8.0, 1.0)
+        cum = np.cumsum(work)
+        cuts = [0]
+        for g in range(1, self.chunks):
+            k = int(np.searchsorted(cum, cum[-1] * g / self.chunks))
+            if k > cuts[-1]:
+                cuts.append(k)
+        cuts.append(len(instances))
+        return [(a, b) for a, b in zip(cuts, cuts[1:]) if b > a]
+
+    def evaluate(self, instances):
+        import torch
+        instances = list(instances)
+        if not instances:
+            return []
+        keep, outs, self.h2d_bytes, self.d2h_bytes = [], [], 0, 0
+        for a, b in self.groups(instances):
+            stream = self.compute
+            with torch.cuda.stream(stream):
+                batch = Batch(instances[a:b], plan_cache=self.plans, staging=self._pinned, **self.kw)
+                batch.run()
+                done = torch.cuda.Event()
+                done.record(stream)
+            self.copy.wait_event(done)
+            host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+                    for t in (batch.time, batch.u, batch.state, batch.spin)]
+            with torch.cuda.stream(self.copy):
+                for h, t in zip(host, (batch.time, batch.u, batch.state, batch.spin)):
+                    h.copy_(t, non_blocking=True)
+            keep.append(batch)
+            outs.append((batch, [h.numpy() for h in host], host))
+            self.h2d_bytes += batch.h2d_bytes
+            self.d2h_bytes += sum(h.numel() * h.element_size() for h in host)
+        self.copy.synchronize()
+        del keep
+        return HostResults([(batch._inst_np.copy(), arrays, host) for batch, arrays, host in outs])
+
+
+class HostResults:
+    """The ``Results`` of an ``Evaluator.evaluate`` call, in instance order: a sequence whose items
+    are made on access from page-locked host arrays that already hold every output."""
+
+    def __init__(self, groups):
+        self._groups = groups
+        self._index = []
+        for g, (desc, _, _) in enumerate(groups):
+            self._index += [(g, k) for k in range(len(desc))]
+
+    def __len__(self):
+        return len(self._index)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(len(self)))]
+        g, k = self._index[i]
+        desc, (time, u, state, spin), host = self._groups[g]
+        r = desc[k]
+        out_off, u_off, st_off = int(r["out_offset"]), int(r["u_offset"]), int(r["state_offset"])
+        n_out, d = int(r["n_out"]), int(r["dim"])
+        return Results(time[out_off:out_off + n_out], u[u_off // 2:u_off // 2 + n_out * d * d].reshape(n_out, d, d),
+                       state[st_off // 2:st_off // 2 + n_out * d].reshape(n_out, d), None,
+                       spin=spin[out_off:out_off + n_out], keep=host)
+
+    def __iter__(self):
+        return (self[i] for i in range(len(self)))
+
+
+def evaluate_many(instances, chunks=6, **batch_kwargs):
+    """Evaluate a list of instances (see ``Instance``) into host ``Results`` with set-up, kernels
+    and device-to-host copies overlapped across ``chunks`` groups (``Evaluator``)."""
+    return Evaluator(chunks=chunks, **batch_kwargs).evaluate(instances)

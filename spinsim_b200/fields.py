@@ -100,6 +100,16 @@ class TabulatedField(BuiltinField):
     def uses_channel(self, c):
         return c in self.tables or self.bias[c] != 0.0
 
+    def packed_doubles(self):
+        """float64 entries in a packed field buffer: times (shared between channels) and
+        amplitudes padded to 32 bytes, and eight 32-byte table descriptors."""
+        if "_packed_doubles" not in self.__dict__:
+            times = {id(t): t.size for t, _, _, _ in self.tables.values()}
+            n = sum((m + 3) // 4 * 4 for m in times.values())
+            n += sum((a.size + 3) // 4 * 4 for _, a, _, _ in self.tables.values())
+            self._packed_doubles = n + 8 * _TABLE_DOUBLES
+        return self._packed_doubles
+
 
 class ToneField(BuiltinField):
     """channel c = bias[c] + sum_k A_k sin(w_k t + phi_k).
@@ -112,7 +122,7 @@ class ToneField(BuiltinField):
     def __init__(self, tones, bias=None):
         self.tones = {}
         for c, arr in dict(tones).items():
-            arr = np.asarray(arr, np.float64).reshape(-1, 3)
+            arr = np.array(arr, np.float64).reshape(-1, 3)  # a snapshot
             self.tones[_channel_index(c)] = arr
         self.bias = np.zeros(8)
         if bias is not None:
@@ -120,7 +130,12 @@ class ToneField(BuiltinField):
                 self.bias[_channel_index(c)] = v
 
     def packed(self):
-        """(flat (w, A, phi) array, start[8], count[8])."""
+        """(flat (w, A, phi) array, start[8], count[8]), computed once (the tones are snapshots)."""
+        if "_packed" not in self.__dict__:
+            self._packed = self._pack()
+        return self._packed
+
+    def _pack(self):
         start = np.zeros(8, np.int32)
         count = np.zeros(8, np.int32)
         rows = []
@@ -151,6 +166,22 @@ class ToneField(BuiltinField):
     def uses_channel(self, c):
         return c in self.tones or self.bias[c] != 0.0
 
+    def packed_doubles(self):
+        """float64 entries in a packed field buffer: the (w, A, phi) rows padded to 32 bytes."""
+        return (self.packed()[0].size + 3) // 4 * 4 or 4
+
+    def field_record(self):
+        """The field's spinsim_field struct without its tone pointer (computed once)."""
+        if "_record" not in self.__dict__:
+            rec = np.zeros((), FIELD_DTYPE)
+            _, start, count = self.packed()
+            rec["tone_start"] = start
+            rec["tone_count"] = count
+            rec["bias"] = self.bias
+            rec["gain"] = 1.0
+            self._record = rec
+        return self._record
+
     def sample(self, t):
         """Host evaluation (for plots and checks): array of shape (len(t), 8)."""
         t = np.atleast_1d(np.asarray(t, np.float64))
@@ -176,15 +207,7 @@ def packed_doubles(fields):
     its times and amplitudes, each padded to 32 bytes, and eight 32-byte table descriptors per
     tabulated field; the (w, A, phi) rows of a tone field padded to 32 bytes."""
     _check_fields(fields)
-    total = 0
-    for f in fields:
-        if isinstance(f, TabulatedField):
-            times = {id(t): t.size for t, _, _, _ in f.tables.values()}
-            total += sum((m + 3) // 4 * 4 for m in times.values())
-            total += sum((a.size + 3) // 4 * 4 for _, a, _, _ in f.tables.values()) + 8 * _TABLE_DOUBLES
-        else:
-            total += (3 * sum(a.shape[0] for a in f.tones.values()) + 3) // 4 * 4 or 4
-    return total
+    return sum(f.packed_doubles() for f in fields)
 
 
 def pack_fields_into(fields, host, base):
@@ -236,16 +259,13 @@ def pack_fields_into(fields, host, base):
         out["gain"] = np.stack([f.gain for f in fields])
     else:
         starts = []
-        for k, f in enumerate(fields):
-            flat, start, count = f.packed()
+        for f in fields:
+            flat = f.packed()[0]
             host[at:at + flat.size] = flat
             starts.append(at)
-            out["tone_start"][k] = start
-            out["tone_count"][k] = count
             at += (flat.size + 3) // 4 * 4 or 4
+        out[:] = [f.field_record() for f in fields]
         out["tones"] = base + 8 * np.array(starts, np.uint64)
-        out["bias"] = np.stack([f.bias for f in fields])
-        out["gain"] = 1.0
     return out
 
 

@@ -167,8 +167,7 @@ class Server:
         self.arena = Arena(self.hbm_budget)
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         # pinned host staging for each stream's field upload (reused once the stream's launch is done)
-        self.staging = [torch.empty(int(staging_bytes) // 8, dtype=torch.float64, pin_memory=True)
-                        for _ in range(streams)]
+        self.staging = [torch.empty(int(staging_bytes), dtype=torch.uint8, pin_memory=True) for _ in range(streams)]
         self.max_batch = max_batch
         self.copy_to_host = copy_to_host
         self.kw = dict(precision=self.precision, number_of_squares=number_of_squares, lanes=1,
