@@ -24,8 +24,11 @@ bit for bit.  Latency is measured on the host clock from arrival to completion.
 """
 import bisect
 import collections
+import concurrent.futures
 import gc
 import math
+import queue as queue_mod
+import threading
 import time
 import weakref
 from dataclasses import dataclass, field as dc_field
@@ -151,6 +154,19 @@ class ArenaFull(Exception):
     pass
 
 
+class BudgetHeld(RuntimeError):
+    """Nothing is running and the next request does not fit: results still referenced hold the arena."""
+
+
+class LaunchError(Exception):
+    """A launch could not be made; ``requests`` were taken from the queue for it."""
+
+    def __init__(self, requests, error):
+        super().__init__(str(error))
+        self.requests = requests
+        self.error = error
+
+
 class Server:
     """Continuous-batching evaluator.  ``hbm_budget`` bytes of HBM (one arena, taken at start-up)
     hold the outputs and scratch of launches in flight and of results the caller still holds; up to
@@ -224,6 +240,8 @@ class Server:
         gc.disable()  # a full collection over the live results would stall the loop for tens of ms
         try:
             return self._run(pending, clock, idle_sleep, on_complete, keep_results)
+        except LaunchError as e:
+            raise e.error
         finally:
             if gc_was_enabled:
                 gc.enable()
@@ -250,6 +268,93 @@ class Server:
                 else:
                     time.sleep(idle_sleep)
         return done
+
+    # ------------------------------------------------------------------ asynchronous serving
+    def start(self):
+        """Serve submitted requests on a background thread (``submit`` returns futures)."""
+        import torch
+        if getattr(self, "_thread", None) is not None:
+            raise RuntimeError("the server is already running")
+        self._inbox = queue_mod.SimpleQueue()
+        self._stopping = threading.Event()
+        self._t0 = time.perf_counter()
+        self._error = None
+        device = torch.cuda.current_device()
+        self._thread = threading.Thread(target=self._serve_forever, args=(device,), name="spinsim-server", daemon=True)
+        self._thread.start()
+        return self
+
+    def submit(self, request):
+        """Queue ``request`` (a ``Request``; its arrival is now) and return a
+        ``concurrent.futures.Future`` that resolves to its ``Results`` (views of the arena, which the
+        request's block holds until they are released) or to the launch's exception."""
+        if getattr(self, "_thread", None) is None or self._stopping.is_set():
+            raise RuntimeError("the server is not running: call start()")
+        if request.footprint() > self.arena.size:
+            raise ValueError(f"request {request.id} needs {request.footprint()} bytes, above the HBM budget")
+        future = concurrent.futures.Future()
+        request.arrival = time.perf_counter() - self._t0
+        self._inbox.put((request, future))
+        return future
+
+    def close(self, wait=True):
+        """Stop accepting requests, finish the queued and running ones, and stop the thread."""
+        thread = getattr(self, "_thread", None)
+        if thread is None:
+            return
+        self._stopping.set()
+        if wait:
+            thread.join()
+        self._thread = None
+        if self._error is not None:
+            raise self._error
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _serve_forever(self, device, idle_sleep=20e-6):
+        import torch
+        torch.cuda.set_device(device)
+        futures = {}
+        queue = collections.deque()
+        inflight = []
+        free_streams = list(range(len(self.streams)))
+        clock = time.perf_counter
+        t0 = self._t0
+
+        def resolve(c):
+            futures.pop(id(c.request)).set_result(c.results)
+
+        try:
+            while True:
+                while True:
+                    try:
+                        req, fut = self._inbox.get_nowait()
+                    except queue_mod.Empty:
+                        break
+                    if fut.set_running_or_notify_cancel():
+                        futures[id(req)] = fut
+                        queue.append(req)
+                inflight = self._complete(inflight, free_streams, [], clock, t0, resolve, False)
+                while queue and free_streams:
+                    try:
+                        if not self._admit(queue, inflight, free_streams, clock, t0):
+                            break
+                    except LaunchError as e:  # a launch that cannot be made fails its requests
+                        for r in e.requests:
+                            futures.pop(id(r)).set_exception(e.error)
+                    except BudgetHeld as e:  # the head request cannot run until results are released
+                        futures.pop(id(queue.popleft())).set_exception(e)
+                if self._stopping.is_set() and not queue and not inflight and self._inbox.empty():
+                    break
+                time.sleep(idle_sleep)
+        except Exception as e:  # pragma: no cover - reported by close()
+            self._error = e
+            for fut in futures.values():
+                fut.set_exception(e)
 
     def _complete(self, inflight, free_streams, done, clock, t0, on_complete, keep_results):
         """Resolve the launches whose event has passed; returns the launches still running."""
@@ -292,8 +397,8 @@ class Server:
             if not inflight:
                 gc.collect()  # results released only through a reference cycle
                 if self.arena.largest_free() < queue[0].footprint():
-                    raise RuntimeError("the HBM budget is held by results still referenced: release Results "
-                                       "(or serve with keep_results=False) or raise hbm_budget")
+                    raise BudgetHeld("the HBM budget is held by results still referenced: release Results "
+                                     "(or serve with keep_results=False) or raise hbm_budget")
                 return True
             return False
         si = free_streams.pop()
@@ -313,6 +418,9 @@ class Server:
                 half = len(take) // 2
                 queue.extendleft(reversed(take[half:]))
                 take = take[:half]
+            except Exception as e:
+                free_streams.append(si)
+                raise LaunchError(take, e) from e
         inflight.append((b, ev, take, si, clock() - t0))
         self.stats["admitted"] += len(take)
         return True

@@ -99,3 +99,24 @@ def test_footprint_bounds_the_launch(cuda):
     for group in (reqs[:1], reqs[1:2], reqs[:8], reqs):
         b = Batch([r.instance() for r in group], **srv.kw)
         assert b.device_bytes <= sum(r.footprint() for r in group)
+
+
+def test_async_submit_futures(cuda):
+    """start/submit/close: futures resolve to the same results as a synchronous run, and a request
+    whose launch cannot be made fails its own future."""
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Request, Server
+    reqs = requests(n=16, rate=1e5, seed=21)
+    sync = {c.request.id: c.results for c in Server(precision=ss.Precision.FP64, streams=2).run(reqs)}
+    with Server(precision=ss.Precision.FP64, streams=3, max_batch=4) as srv:
+        bad = Request(ss.SpinQuantumNumber.HALF, reqs[0].field, 0.0, 20e-6, 1e-7, 1e-6, [1.0, 0.0, 0.0], id=-1)
+        bad_future = srv.submit(bad)
+        with pytest.raises(ValueError):
+            bad_future.result(timeout=60)
+        futures = [srv.submit(r) for r in reqs]
+        got = [f.result(timeout=120) for f in futures]
+    for r, res in zip(reqs, got):
+        assert np.array_equal(res.state, sync[r.id].state)
+        assert np.array_equal(res.time_evolution, sync[r.id].time_evolution)
+    with pytest.raises(RuntimeError):
+        srv.submit(reqs[0])  # closed
