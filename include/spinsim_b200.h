@@ -105,7 +105,9 @@ typedef struct {
     int32_t n_fine;
     int32_t dim;
     int32_t field;  /* index into the batch's field array */
-    int32_t reserved;
+    int32_t interval0; /* time index of this instance's output step 0: time[i] = t0 + dt_out * (interval0 + i),
+                        * as in I:818; 0 for a whole evaluate(), the first index of a piece when one
+                        * evaluate() is split across launches or GPUs */
     double psi0[6]; /* complex[dim] interleaved */
 } spinsim_instance;
 
@@ -172,6 +174,20 @@ int spinsim_state(int32_t dim, const double* u_dev, int64_t n_out, const double*
 int64_t spinsim_state_static_max_steps(void);
 int spinsim_state_static(int32_t dim, const double* u_dev, int64_t n_out, const double* psi0, double* state_dev,
                          double* spin_dev, void* stream);
+
+/* One evaluate() split into pieces of consecutive output steps (across launches or GPUs; no
+ * counterpart in the reference, whose get_state I:1087-1111 is one serial loop).  For a piece with
+ * operators u_dev[n][d][d] (computed with spinsim_instance.interval0 = the piece's first time index):
+ *   spinsim_piece_product writes P = U[n-1] ... U[0] (complex [d][d]) to product_dev and leaves the
+ *   piece's prefixes in the workspace (spinsim_state_workspace_size(dim, n) bytes);
+ *   spinsim_piece_states, given psi_in = the state entering the piece (the pieces before it applied to
+ *   psi0, in order), writes state[i] = U[i-1] ... U[0] psi_in and spin from the prefixes left in the
+ *   same workspace by spinsim_piece_product on the same u_dev, and must follow it on the stream.
+ * The state entering piece r is P_{r-1} ... P_0 psi0: one exchange of d x d products between pieces. */
+int spinsim_piece_product(int32_t dim, const double* u_dev, int64_t n_out, double* product_dev, void* workspace_dev,
+                          size_t workspace_bytes, void* stream);
+int spinsim_piece_states(int32_t dim, const double* u_dev, int64_t n_out, const double* psi_in, double* state_dev,
+                         double* spin_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
 
 /* get_spin alone (I:899-959; spin_calculator I:961-988): spin_dev[N][3] from state_dev[N][d]. */
 int spinsim_spin(int32_t dim, const double* state_dev, int64_t n_out, double* spin_dev, void* stream);

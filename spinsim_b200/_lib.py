@@ -41,7 +41,7 @@ class Field(ctypes.Structure):
 class Instance(ctypes.Structure):
     _fields_ = [("t0", c_dbl), ("dt_int", c_dbl), ("dt_out", c_dbl), ("n_out", c_i64), ("out_offset", c_i64),
                 ("u_offset", c_i64), ("state_offset", c_i64), ("n_fine", c_i32), ("dim", c_i32), ("field", c_i32),
-                ("reserved", c_i32), ("psi0", c_dbl * 6)]
+                ("interval0", c_i32), ("psi0", c_dbl * 6)]
 
 
 class PlanInfo(ctypes.Structure):
@@ -84,6 +84,8 @@ _SIGNATURES = [
     ("spinsim_batch_workspace_size", ctypes.c_size_t, [c_vp, ctypes.POINTER(Instance), c_i32, c_i32]),
     ("spinsim_batch_prepare", ctypes.c_int,
      [c_vp, ctypes.POINTER(Instance), c_i32, c_vp, c_i32, c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
+    ("spinsim_piece_product", ctypes.c_int, [c_i32, c_vp, c_i64, c_vp, c_vp, ctypes.c_size_t, c_vp]),
+    ("spinsim_piece_states", ctypes.c_int, [c_i32, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     ("spinsim_batch_staging_size", ctypes.c_size_t, [c_vp, ctypes.POINTER(Instance), c_i32, c_i32]),
     ("spinsim_batch_prepare_staged", ctypes.c_int,
      [c_vp, ctypes.POINTER(Instance), c_i32, c_vp, c_i32, c_vp, ctypes.c_size_t, c_vp, ctypes.c_size_t, c_vp,

@@ -34,6 +34,9 @@ class Instance:
     sweep_parameters: Sequence[float] = (0.0,)
     field: Optional[BuiltinField] = None
     meta: dict = dc_field(default_factory=dict)
+    # (first, count): compute only output steps first .. first + count - 1 of this evaluate()
+    # (one piece of a split evaluation; time indices stay those of the whole call)
+    intervals: Optional[tuple] = None
 
 
 class Batch:
@@ -135,6 +138,8 @@ class Batch:
                                               dims.ctypes.data, psi0.ctypes.data, insts, totals))
         out_off, u_off, st_off, self.total_steps = (int(v) for v in totals)
         self._inst_np = np.frombuffer(insts, dtype=np.dtype(_lib.Instance))
+        if any(getattr(i, "intervals", None) is not None for i in self.instances):
+            out_off, u_off, st_off = self._restrict_to_pieces()
         keep = []
         params_host = []
         if get_field is not None:
@@ -253,6 +258,26 @@ class Batch:
         info = _lib.PlanInfo()
         _lib.check(self.lib.spinsim_plan_get_info(self._plan, ctypes.byref(info)))
         return {k: getattr(info, k) for k, _ in _lib.PlanInfo._fields_}
+
+    def _restrict_to_pieces(self):
+        """Apply the instances' ``intervals`` (first, count) to the descriptors and re-pack the
+        output offsets; returns the new totals (output steps, U doubles, state doubles)."""
+        rec = self._inst_np
+        for k, inst in enumerate(self.instances):
+            if inst.intervals is None:
+                continue
+            first, count = (int(v) for v in inst.intervals)
+            if first < 0 or count < 0 or first + count > rec[k]["n_out"] or first >= 2 ** 31:
+                raise ValueError(f"instance {k}: output steps {first}..{first + count} are outside 0..{rec[k]['n_out']}")
+            rec[k]["n_out"] = count
+            rec[k]["interval0"] = first
+        n_out = rec["n_out"].astype(np.int64)
+        d = rec["dim"].astype(np.int64)
+        for name, per in (("out_offset", n_out), ("u_offset", 2 * d * d * n_out), ("state_offset", 2 * d * n_out)):
+            rec[name][0] = 0
+            rec[name][1:] = np.cumsum(per)[:-1]
+        self.total_steps = int((n_out * rec["n_fine"]).sum())
+        return int(n_out.sum()), int((2 * d * d * n_out).sum()), int((2 * d * n_out).sum())
 
     def layout_of(self, k):
         """(output offset, U offset, state offset (in doubles), N, d) of instance k."""

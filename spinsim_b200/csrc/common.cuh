@@ -68,7 +68,7 @@ struct Instance {
     int32_t n_fine;       // K = floor(dt_out / dt_int + 0.5)  (I:832)
     int32_t dim;          // 2 or 3
     int32_t field;        // index into the FieldDesc array
-    int32_t pad;
+    int32_t interval0;    // time index of output interval 0: time[i] = t0 + dt_out * (interval0 + i)
     double psi0[6];       // initial state, complex[dim] interleaved
 };
 

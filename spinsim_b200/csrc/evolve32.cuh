@@ -233,7 +233,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lanes = m.lanes;
     const double dt = inst.dt_int, dt_out = inst.dt_out;
-    const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)index));  // I:818, unfused
+    const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)(inst.interval0 + index)));  // I:818, unfused
     double s0[8], s1[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -411,7 +411,7 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
     for (int i = 0; i < NI; i++) {
         active[i] = lane + 32 * i < tile.count;
         index[i] = tile.first + (active[i] ? lane + 32 * i : 0);
-        t_c[i] = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)index[i]));  // I:818, unfused
+        t_c[i] = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)(inst.interval0 + index[i])));  // I:818, unfused
         rw[i] = 0.0;
         W[i] = Wrot[i] = Woff[i] = c64{1.0, 0.0};
         if (active[i] && m.rotating) {
@@ -455,8 +455,8 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
             sincos(w * dt, &rg[1], &rg[0]);
             sincos(w * (a_hi - a_lo), &rg[3], &rg[2]);
             // G = exp(i w (t_c(l + 32) - t_c(l))), t_c rounded as the intervals' own starts are
-            sincos(w * (__dmul_rn(dt_out, (double)(index[0] + 32)) - __dmul_rn(dt_out, (double)index[0])),
-                   &rg[5], &rg[4]);
+            const int64_t i0 = inst.interval0 + index[0];
+            sincos(w * (__dmul_rn(dt_out, (double)(i0 + 32)) - __dmul_rn(dt_out, (double)i0)), &rg[5], &rg[4]);
         }
 #pragma unroll
         for (int q = 0; q < 6; q++) ts->rg[lane][q] = rg[q];

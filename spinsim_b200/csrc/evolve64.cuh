@@ -81,7 +81,7 @@ SS_D void interval64(const MethodConfig& m, const Instance& inst, const FieldDes
     const int lanes = m.lanes;
     const double dt = inst.dt_int, dt_out = inst.dt_out;
     // I:818, rounded as the reference rounds it (no fused multiply-add), so time[] is bit-exact
-    const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)index));
+    const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)(inst.interval0 + index)));
     double s0[8], s1[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) s0[k] = 0.0;

@@ -9,7 +9,7 @@
 //      thread products in shared memory and stores each thread's exclusive in-tile prefix and the
 //      tile product.
 //   B  scan_tiles_kernel: one thread per instance walks its tiles in order and stores the
-//      exclusive prefix of every tile.
+//      exclusive prefix of every tile (and, when asked, the instance's whole product).
 //   C  scan_apply_kernel: thread t forms prefix = (in-tile prefix) (tile prefix), applies it to psi0
 //      and walks its chunk writing state and spin (get_spin, I:899-959), fused.
 #pragma once
@@ -76,6 +76,7 @@ struct ScanArgs {
     double* tile_prefix;      // [n_tiles][D][D] complex
     double* state;            // complex [sum N * d]
     double* spin;             // [sum N * 3], may be null
+    double* total;            // per instance (of this dim): U[N-1] ... U[0], complex [D][D]; may be null
 };
 
 template <int D>
@@ -140,6 +141,7 @@ __global__ void scan_tiles_kernel(ScanArgs a) {
         store_mat<D>(a.tile_prefix + (int64_t)k * MD, run);
         run = matmul(load_mat<D>(a.tile_product + (int64_t)k * MD), run);
     }
+    if (a.total) store_mat<D>(a.total + (int64_t)i * MD, run);
 }
 
 template <int D>
