@@ -189,6 +189,16 @@ int spinsim_piece_product(int32_t dim, const double* u_dev, int64_t n_out, doubl
 int spinsim_piece_states(int32_t dim, const double* u_dev, int64_t n_out, const double* psi_in, double* state_dev,
                          double* spin_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
 
+/* Ensemble mean of the spin on the device (no counterpart in the reference, whose users average
+ * Results.spin on the host after copying every member's states back): for members m = 0 .. members-1
+ * whose spin series start at output step first + m * stride of spin_dev (e.g. the instances of a
+ * batch with equal N: first = out_offset of the first, stride = N), mean_dev[i][c] = the average
+ * over members of spin[first + m * stride + i][c], i < n_out.  The sum runs in a fixed order (chunks
+ * of members, then the chunks in order).  Workspace: spinsim_spin_mean_workspace_size bytes. */
+size_t spinsim_spin_mean_workspace_size(int32_t members, int64_t n_out);
+int spinsim_spin_mean(const double* spin_dev, int64_t first, int64_t stride, int32_t members, int64_t n_out,
+                      double* mean_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
+
 /* get_spin alone (I:899-959; spin_calculator I:961-988): spin_dev[N][3] from state_dev[N][d]. */
 int spinsim_spin(int32_t dim, const double* state_dev, int64_t n_out, double* spin_dev, void* stream);
 

@@ -299,12 +299,42 @@ class Batch:
         return Results(time, u, st, None, spin=sp, keep=keep)
 
     def final_states(self):
-        """state[N-1] of every instance as a list of numpy arrays."""
-        st = self.state.cpu().numpy()
-        out = []
-        for out_off, u_off, st_off, n_out, d in map(self.layout_of, range(len(self.instances))):
-            out.append(st[st_off // 2 + (n_out - 1) * d: st_off // 2 + n_out * d] if n_out else np.zeros(d, complex))
+        """state[N-1] of every instance as a list of numpy arrays (gathered on the device, so only
+        the final states are copied to the host)."""
+        import torch
+        rec = self._inst_np
+        n_out = rec["n_out"].astype(np.int64)
+        d = rec["dim"].astype(np.int64)
+        start = rec["state_offset"].astype(np.int64) // 2 + np.maximum(n_out - 1, 0) * d
+        idx = np.concatenate([np.arange(s, s + k) for s, k in zip(start, d)]) if len(d) else np.zeros(0, np.int64)
+        got = self.state[torch.from_numpy(idx).to(self.state.device)].cpu().numpy()
+        out, at = [], 0
+        for k in range(len(d)):
+            out.append(got[at:at + d[k]].copy() if n_out[k] else np.zeros(d[k], complex))
+            at += d[k]
         return out
+
+    def spin_mean(self, first=0, count=None):
+        """Mean spin over instances first .. first + count - 1, which must share N (the members of
+        an ensemble); a (N, 3) float64 tensor on the device, reduced there (``spinsim_spin_mean``)."""
+        import torch
+        rec = self._inst_np
+        count = len(self.instances) - first if count is None else count
+        if count <= 0 or first < 0 or first + count > len(self.instances):
+            raise ValueError("instance range out of bounds")
+        n = int(rec["n_out"][first])
+        if np.any(rec["n_out"][first:first + count] != n):
+            raise ValueError("the members of a spin mean must share their number of output steps")
+        offs = rec["out_offset"][first:first + count].astype(np.int64)
+        if count > 1 and np.any(np.diff(offs) != n):
+            raise ValueError("the members are not laid out one after another")
+        mean = torch.empty((max(n, 1), 3), dtype=torch.float64, device=self.device)
+        ws_bytes = self.lib.spinsim_spin_mean_workspace_size(count, n)
+        ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.device)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(self.lib.spinsim_spin_mean(self.spin.data_ptr(), int(offs[0]), n, count, n, mean.data_ptr(),
+                                              ws.data_ptr(), ws_bytes, stream))
+        return mean[:n]
 
     def __del__(self):
         try:

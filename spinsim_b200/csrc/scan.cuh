@@ -216,4 +216,41 @@ __global__ void spin_kernel(const double* state, int64_t n, double* spin) {
     spin[i * 3 + 2] = o[2];
 }
 
+// Ensemble mean of the spin over members that share their output times (one evaluate() each,
+// equal N, laid out one after another): mean[i][c] = (1/M) sum_m spin[first + m * stride + i][c].
+// Launch A sums a chunk of members for 128 output steps per CTA (coalesced over i), launch B adds
+// the chunk sums in chunk order, so the result does not depend on the launch shape's timing.
+constexpr int kMeanThreads = 128;
+
+__global__ void __launch_bounds__(kMeanThreads) spin_mean_partial_kernel(const double* spin, int64_t first,
+                                                                         int64_t stride, int32_t members,
+                                                                         int32_t per_chunk, int64_t n_out,
+                                                                         double* partial) {
+    const int64_t i = (int64_t)blockIdx.x * kMeanThreads + threadIdx.x;
+    const int chunk = blockIdx.y;
+    if (i >= n_out) return;
+    const int m0 = chunk * per_chunk;
+    const int m1 = min(members, m0 + per_chunk);
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int m = m0; m < m1; m++) {
+        const double* p = spin + (first + (int64_t)m * stride + i) * 3;
+        sx += __ldg(p);
+        sy += __ldg(p + 1);
+        sz += __ldg(p + 2);
+    }
+    double* q = partial + ((int64_t)chunk * n_out + i) * 3;
+    q[0] = sx;
+    q[1] = sy;
+    q[2] = sz;
+}
+
+__global__ void __launch_bounds__(kMeanThreads) spin_mean_final_kernel(const double* partial, int32_t chunks,
+                                                                       int32_t members, int64_t n_out, double* mean) {
+    const int64_t k = (int64_t)blockIdx.x * kMeanThreads + threadIdx.x;  // (i, c) flattened
+    if (k >= n_out * 3) return;
+    double s = 0.0;
+    for (int c = 0; c < chunks; c++) s += partial[(int64_t)c * n_out * 3 + k];
+    mean[k] = s / (double)members;
+}
+
 }  // namespace spinsim
