@@ -82,9 +82,10 @@ def instances(ss, specs):
 # product 90 in FP32.
 FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
 FLOPS_BULK = {2: {"fp64": 290, "fp32": 90}, 3: {"fp64": 296, "fp32": 90}}
-# DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload, from
-# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum` (1 pass), profiles/evolve_fp32bulk_tones.md.
-TRAFFIC_BYTES_PER_LAUNCH = 1853696 + 81376256
+# DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload
+# (max_registers 168, state scan not run), from one capture of
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve -c 1`.
+TRAFFIC_BYTES_PER_LAUNCH = 1982208 + 81064448
 
 
 def algorithmic_bytes(specs):
@@ -570,9 +571,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         steps, el, frac = cpu_sample(specs, seconds_target=10.0)
+        steps1, el1, frac1 = cpu_sample(specs, seconds_target=3.0, n_threads=1)
         out["cpu_baseline"] = {"value": steps / el, "unit": "steps/s", "cores": O.max_threads(), "kind": "port",
                                "sample": f"oracle (reference algorithm in C, OpenMP) on the first {frac:.4f} of "
-                                         f"the output intervals of every instance: {steps} integration steps"}
+                                         f"the output intervals of every instance: {steps} integration steps",
+                               "single_core": {"value": steps1 / el1, "unit": "steps/s", "cores": 1,
+                                               "sample": f"first {frac1:.4f} of the output intervals of every "
+                                                         f"instance: {steps1} integration steps"}}
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -251,3 +251,28 @@ def test_spin_mean_rejects_unequal_members(cuda):
     b.run()
     with pytest.raises(ValueError):
         b.spin_mean()
+
+
+def test_ragged_batch_edge_instances(cuda):
+    """A batch mixing an empty instance (t1 == t0), a single output step, K = 1 (dt_int = dt_out), a
+    non-integer step ratio (dt_int reset as the reference does) and fewer steps than a warp, against
+    the oracle; the empty instance yields empty arrays."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    H, O1 = ss.SpinQuantumNumber.HALF, ss.SpinQuantumNumber.ONE
+    p = F.tone_parameters(np.random.default_rng(77))
+    specs = [(H, 0.0, 0.0, 10e-9, 1e-6), (H, 0.0, 1e-6, 10e-9, 1e-6), (O1, 0.0, 20e-6, 1e-6, 1e-6),
+             (H, 1e-6, 31e-6, 30e-9, 1e-6), (O1, 0.0, 7e-6, 10e-9, 1e-6), (H, 0.0, 200e-6, 10e-9, 1e-6)]
+    insts = [B.Instance(s, t0, t1, dti, dto, s.plus_x, sweep_parameters=p, field=tone_field(p))
+             for s, t0, t1, dti, dto in specs]
+    for prec in (ss.Precision.FP64, ss.Precision.FP32_BULK):
+        b = B.Batch(insts, precision=prec)
+        b.run()
+        for k, (s, t0, t1, dti, dto) in enumerate(specs):
+            r = b.result(k)
+            t, u, st, sp = O.evaluate(s.dimension, O.Field(8), p, t0, t1, dti, dto, s.plus_x)
+            assert r.time.shape == t.shape and r.state.shape == st.shape
+            assert np.array_equal(r.time, t)
+            if t.size:
+                tol = 1e-10 if prec == ss.Precision.FP64 else 1e-6
+                assert np.abs(r.state - st).max() < tol, (prec, k)
