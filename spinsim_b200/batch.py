@@ -305,13 +305,17 @@ class Batch:
         rec = self._inst_np
         n_out = rec["n_out"].astype(np.int64)
         d = rec["dim"].astype(np.int64)
-        start = rec["state_offset"].astype(np.int64) // 2 + np.maximum(n_out - 1, 0) * d
-        idx = np.concatenate([np.arange(s, s + k) for s, k in zip(start, d)]) if len(d) else np.zeros(0, np.int64)
-        got = self.state[torch.from_numpy(idx).to(self.state.device)].cpu().numpy()
+        start = rec["state_offset"].astype(np.int64) // 2 + (n_out - 1) * d
+        full = np.flatnonzero(n_out > 0)  # an empty instance has no final state (and no entries to read)
+        idx = np.concatenate([np.arange(start[k], start[k] + d[k]) for k in full]) if len(full) else None
+        got = self.state[torch.from_numpy(idx).to(self.state.device)].cpu().numpy() if idx is not None else None
         out, at = [], 0
         for k in range(len(d)):
-            out.append(got[at:at + d[k]].copy() if n_out[k] else np.zeros(d[k], complex))
-            at += d[k]
+            if n_out[k]:
+                out.append(got[at:at + d[k]].copy())
+                at += d[k]
+            else:
+                out.append(np.zeros(d[k], complex))
         return out
 
     def spin_mean(self, first=0, count=None):

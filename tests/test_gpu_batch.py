@@ -276,3 +276,7 @@ def test_ragged_batch_edge_instances(cuda):
             if t.size:
                 tol = 1e-10 if prec == ss.Precision.FP64 else 1e-6
                 assert np.abs(r.state - st).max() < tol, (prec, k)
+        finals = b.final_states()  # the empty instance has none to gather
+        assert np.array_equal(finals[0], np.zeros(2, complex))
+        for k in range(1, len(specs)):
+            assert np.array_equal(finals[k], b.result(k).state[-1])
