@@ -384,13 +384,23 @@ def measured_fp64_peak():
 
 
 # ------------------------------------------------------------------------------------ reference arm
+def host_threads():
+    """Host cores this process may run on (torchrun sets OMP_NUM_THREADS=1 for its workers, so the
+    CPU arms pass this count to the oracle explicitly)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def bench_reference(args, world, rank):
     from oracle import oracle as O
     specs = workload(seed_base=0)
     O.lib()
-    threads = O.max_threads()
+    threads = host_threads()
     times, steps_list = [], []
-    _, _, frac = cpu_sample(specs, seconds_target=min(8.0, 120.0 / max(1, args.steps + args.warmup)))
+    _, _, frac = cpu_sample(specs, seconds_target=min(8.0, 120.0 / max(1, args.steps + args.warmup)),
+                            n_threads=threads)
     field = O.Field(8)
     for it in range(args.warmup + args.steps):
         steps = 0
@@ -399,7 +409,7 @@ def bench_reference(args, world, rank):
             n = int(dur / 1e-6)
             cnt = max(1, int(n * frac)) if n else 0
             if cnt:
-                O.time_evolution(dim, field, p, 0.0, 10e-9, 1e-6, n, first=0, count=cnt)
+                O.time_evolution(dim, field, p, 0.0, 10e-9, 1e-6, n, first=0, count=cnt, n_threads=threads)
                 steps += cnt * 100
         el = time.perf_counter() - t0
         if it >= args.warmup:
@@ -570,9 +580,9 @@ def main():
     out, specs = bench_ours(args, world, rank)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
-        steps, el, frac = cpu_sample(specs, seconds_target=10.0)
+        steps, el, frac = cpu_sample(specs, seconds_target=10.0, n_threads=host_threads())
         steps1, el1, frac1 = cpu_sample(specs, seconds_target=3.0, n_threads=1)
-        out["cpu_baseline"] = {"value": steps / el, "unit": "steps/s", "cores": O.max_threads(), "kind": "port",
+        out["cpu_baseline"] = {"value": steps / el, "unit": "steps/s", "cores": host_threads(), "kind": "port",
                                "sample": f"oracle (reference algorithm in C, OpenMP) on the first {frac:.4f} of "
                                          f"the output intervals of every instance: {steps} integration steps",
                                "single_core": {"value": steps1 / el1, "unit": "steps/s", "cores": 1,
