@@ -441,8 +441,11 @@ def bench_serving(args):
            "precision": "fp32_bulk", "hbm_budget_gb": args.hbm_budget_gb, "rates": {}}
     for rate in rates:
         reqs = synthetic_requests(args.requests, rate, seed=4)
+        kw = {"max_registers": args.max_registers} if args.max_registers > 0 else {}
+        if args.max_steps_per_launch > 0:
+            kw["max_steps_per_launch"] = args.max_steps_per_launch
         srv = Server(precision=ss.Precision.FP32_BULK, hbm_budget=int(args.hbm_budget_gb * (1 << 30)),
-                     streams=args.streams, max_batch=args.max_batch)
+                     streams=args.streams, max_batch=args.max_batch, **kw)
         torch.cuda.synchronize()
         done = srv.run(reqs, keep_results=False)  # the client drops each result as it completes
         torch.cuda.synchronize()
@@ -552,8 +555,9 @@ def main():
     ap.add_argument("--e2e-chunks", type=int, default=6, help="groups overlapped in the end-to-end measurement")
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=20000)
-    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--streams", type=int, default=8)
     ap.add_argument("--max-batch", type=int, default=2048)
+    ap.add_argument("--max-steps-per-launch", type=float, default=0, help="serving: work cap of one launch")
     ap.add_argument("--hbm-budget-gb", type=float, default=16.0)
     args = ap.parse_args()
     world, rank, local = dist_setup()

@@ -101,14 +101,33 @@ class TabulatedField(BuiltinField):
         return c in self.tables or self.bias[c] != 0.0
 
     def packed_doubles(self):
-        """float64 entries in a packed field buffer: times (shared between channels) and
-        amplitudes padded to 32 bytes, and eight 32-byte table descriptors."""
-        if "_packed_doubles" not in self.__dict__:
-            times = {id(t): t.size for t, _, _, _ in self.tables.values()}
-            n = sum((m + 3) // 4 * 4 for m in times.values())
-            n += sum((a.size + 3) // 4 * 4 for _, a, _, _ in self.tables.values())
-            self._packed_doubles = n + 8 * _TABLE_DOUBLES
-        return self._packed_doubles
+        """float64 entries in a packed field buffer: eight 4-double table descriptors, then the
+        times (once per distinct time array) and amplitudes."""
+        return 8 * _TABLE_DOUBLES + self._template()[1]
+
+    def _template(self):
+        """The field's part of a packed buffer, computed once (tables are snapshots): (arrays in
+        order, their total entries, rows (channel, time offset, amplitude offset, size, order,
+        zero_boundary) with offsets from the field's first array, spinsim_field record without the
+        table pointer)."""
+        tpl = self.__dict__.get("_tpl")
+        if tpl is None:
+            arrays, rows, at, seen = [], [], 0, {}
+            for c in sorted(self.tables):
+                t, a, o, z = self.tables[c]
+                ti = seen.get(id(t))
+                if ti is None:
+                    ti = seen[id(t)] = at
+                    arrays.append(t)
+                    at += t.size
+                arrays.append(a)
+                rows.append((c, ti, at, t.size, o, int(z)))
+                at += a.size
+            rec = np.zeros((), FIELD_DTYPE)
+            rec["bias"] = self.bias
+            rec["gain"] = self.gain
+            tpl = self._tpl = (arrays, at, np.array(rows, np.int64).reshape(-1, 6), rec)
+        return tpl
 
 
 class ToneField(BuiltinField):
@@ -203,69 +222,60 @@ def _check_fields(fields):
 
 
 def packed_doubles(fields):
-    """float64 entries the fields take in a packed field buffer (``pack_fields_into``): per table
-    its times and amplitudes, each padded to 32 bytes, and eight 32-byte table descriptors per
-    tabulated field; the (w, A, phi) rows of a tone field padded to 32 bytes."""
+    """float64 entries the fields take in a packed field buffer (``pack_fields_into``): per
+    tabulated field eight 4-double table descriptors and its times and amplitudes; per tone field its
+    (w, A, phi) rows."""
     _check_fields(fields)
     return sum(f.packed_doubles() for f in fields)
 
 
 def pack_fields_into(fields, host, base):
     """Write the fields' arrays (and table descriptors) into ``host`` (a float64 array of at least
-    ``packed_doubles(fields)`` entries) for a device copy of ``host`` at address ``base`` (32-byte
-    aligned); returns the ``spinsim_field`` structs as a numpy array of ``FIELD_DTYPE``.  Padding
-    entries are left as they are."""
+    ``packed_doubles(fields)`` entries) for a device copy of ``host`` at address ``base`` (8-byte
+    aligned; the kernels read these arrays one double at a time); returns the ``spinsim_field``
+    structs as a numpy array of ``FIELD_DTYPE``.  Tabulated fields: all descriptors first, then every
+    field's arrays back to back."""
     _check_fields(fields)
     n = len(fields)
-    out = np.zeros(n, FIELD_DTYPE)
     if not n:
+        return np.zeros(0, FIELD_DTYPE)
+    if isinstance(fields[0], TabulatedField):
+        tpls = [f._template() for f in fields]
+        desc_doubles = 8 * _TABLE_DOUBLES * n
+        sizes = np.fromiter((t[1] for t in tpls), np.int64, n)
+        first = np.empty(n, np.int64)
+        first[0] = desc_doubles
+        np.cumsum(sizes[:-1], out=first[1:])
+        first[1:] += desc_doubles
+        total = desc_doubles + int(sizes.sum())
+        host[:desc_doubles] = 0.0
+        arrays = [a for t in tpls for a in t[0]]
+        if arrays:
+            np.concatenate(arrays, out=host[desc_doubles:total])
+        rows = [t[2] for t in tpls]
+        counts = np.fromiter((r.shape[0] for r in rows), np.int64, n)
+        out = np.array([t[3] for t in tpls], FIELD_DTYPE)
+        out["tables"] = base + 8 * (8 * _TABLE_DOUBLES) * np.arange(n, dtype=np.uint64)
+        if counts.sum():
+            r = np.concatenate(rows)
+            owner = np.repeat(np.arange(n), counts)
+            tab = host[:desc_doubles].view(TABLE_DTYPE)
+            slot = 8 * owner + r[:, 0]
+            tab["time"][slot] = base + 8 * (first[owner] + r[:, 1]).astype(np.uint64)
+            tab["amplitude"][slot] = base + 8 * (first[owner] + r[:, 2]).astype(np.uint64)
+            tab["size"][slot] = r[:, 3]
+            tab["order"][slot] = r[:, 4]
+            tab["zero_boundary"][slot] = r[:, 5]
         return out
     at = 0
-    if isinstance(fields[0], TabulatedField):
-        slot, t_at, a_at, size, order, zb, desc = [], [], [], [], [], [], []
-        for f in fields:
-            first = len(slot)
-            written = {}
-            for c, (t, a, o, z) in f.tables.items():
-                m = t.size
-                p = (m + 3) // 4 * 4
-                ti = written.get(id(t))
-                if ti is None:
-                    host[at:at + m] = t
-                    ti = written[id(t)] = at
-                    at += p
-                host[at:at + m] = a
-                slot.append(c)
-                t_at.append(ti)
-                a_at.append(at)
-                size.append(m)
-                order.append(o)
-                zb.append(z)
-                at += p
-            host[at:at + 8 * _TABLE_DOUBLES] = 0.0
-            desc.append(at)
-            for k in range(first, len(slot)):
-                slot[k] += at // _TABLE_DOUBLES
-            at += 8 * _TABLE_DOUBLES
-        tab = host[:at].view(TABLE_DTYPE)
-        slot = np.array(slot, np.int64)
-        tab["time"][slot] = base + 8 * np.array(t_at, np.uint64)
-        tab["amplitude"][slot] = base + 8 * np.array(a_at, np.uint64)
-        tab["size"][slot] = size
-        tab["order"][slot] = order
-        tab["zero_boundary"][slot] = zb
-        out["tables"] = base + 8 * np.array(desc, np.uint64)
-        out["bias"] = np.stack([f.bias for f in fields])
-        out["gain"] = np.stack([f.gain for f in fields])
-    else:
-        starts = []
-        for f in fields:
-            flat = f.packed()[0]
-            host[at:at + flat.size] = flat
-            starts.append(at)
-            at += (flat.size + 3) // 4 * 4 or 4
-        out[:] = [f.field_record() for f in fields]
-        out["tones"] = base + 8 * np.array(starts, np.uint64)
+    starts = []
+    for f in fields:
+        flat = f.packed()[0]
+        host[at:at + flat.size] = flat
+        starts.append(at)
+        at += f.packed_doubles()
+    out = np.array([f.field_record() for f in fields], FIELD_DTYPE)
+    out["tones"] = base + 8 * np.array(starts, np.uint64)
     return out
 
 

@@ -60,12 +60,21 @@ class Request:
                         self.time_step_output, self.state_init, field=self.field)
 
     def steps(self):
-        """Integration steps of the request (N output steps x K fine steps)."""
-        n = max(0, int((float(self.time_end) - float(self.time_start)) / float(self.time_step_output)))
-        k = int(math.floor(float(self.time_step_output) / float(self.time_step_integration) + 0.5))
-        return n * max(k, 1)
+        """Integration steps of the request (N output steps x K fine steps; computed once)."""
+        got = self.meta.get("_steps")
+        if got is None:
+            n = max(0, int((float(self.time_end) - float(self.time_start)) / float(self.time_step_output)))
+            k = int(math.floor(float(self.time_step_output) / float(self.time_step_integration) + 0.5))
+            got = self.meta["_steps"] = n * max(k, 1)
+        return got
 
     def footprint(self):
+        got = self.meta.get("_footprint")
+        if got is None:
+            got = self.meta["_footprint"] = self._footprint()
+        return got
+
+    def _footprint(self):
         """Upper bound on the device bytes the request takes in a launch, even alone in it.
 
         Outputs (time 8, U 16 d^2, state 16 d, spin 24 bytes per output step); the launch workspace
@@ -83,12 +92,26 @@ class Request:
             fld += 8 * self.field.packed()[0].size + 24
         return n * (33 + 16 * d + 19 * d * d) + 4160 * d * d + 6400 + fld
 
-@dataclass
 class Completed:
-    request: Request
-    results: Any
-    admitted: float
-    completed: float
+    """A served request: its ``results`` (made on first access from the launch's arrays), the
+    times it was admitted and completed, and its ``latency`` (completion - arrival)."""
+
+    __slots__ = ("request", "admitted", "completed", "_batch", "_k", "_results")
+
+    def __init__(self, request, batch, k, admitted, completed):
+        self.request, self.admitted, self.completed = request, admitted, completed
+        self._batch, self._k, self._results = batch, k, None
+
+    @property
+    def results(self):
+        if self._results is None and self._batch is not None:
+            self._results = self._batch.result(self._k, keep=self._batch.lease)
+        return self._results
+
+    @results.setter
+    def results(self, value):
+        self._results = value
+        self._batch = None  # releases the launch's arrays (and its arena block) once nothing else holds them
 
     @property
     def latency(self):
@@ -174,9 +197,9 @@ class Server:
     ``max_steps_per_launch`` integration steps each (a longer request runs alone), which bounds how
     long one launch holds the requests admitted with it."""
 
-    def __init__(self, precision=Precision.FP32_BULK, hbm_budget=8 << 30, streams=4, max_batch=4096,
-                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=128,
-                 max_steps_per_launch=400_000_000, warm_up=True, staging_bytes=32 << 20):
+    def __init__(self, precision=Precision.FP32_BULK, hbm_budget=8 << 30, streams=8, max_batch=4096,
+                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=80,
+                 max_steps_per_launch=100_000_000, warm_up=True, staging_bytes=32 << 20):
         import torch
         self.precision = Precision(precision)
         self.hbm_budget = int(hbm_budget)
@@ -366,7 +389,7 @@ class Server:
                 continue
             tdone = clock() - t0
             for k, r in enumerate(reqs):
-                c = Completed(r, b.result(k, keep=b.lease), adm, tdone)
+                c = Completed(r, b, k, adm, tdone)
                 if on_complete is not None:
                     on_complete(c)
                 if not keep_results:
