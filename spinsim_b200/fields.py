@@ -108,8 +108,7 @@ class TabulatedField(BuiltinField):
     def _template(self):
         """The field's part of a packed buffer, computed once (tables are snapshots): (arrays in
         order, their total entries, rows (channel, time offset, amplitude offset, size, order,
-        zero_boundary) with offsets from the field's first array, spinsim_field record without the
-        table pointer)."""
+        zero_boundary) with offsets from the field's first array)."""
         tpl = self.__dict__.get("_tpl")
         if tpl is None:
             arrays, rows, at, seen = [], [], 0, {}
@@ -123,10 +122,7 @@ class TabulatedField(BuiltinField):
                 arrays.append(a)
                 rows.append((c, ti, at, t.size, o, int(z)))
                 at += a.size
-            rec = np.zeros((), FIELD_DTYPE)
-            rec["bias"] = self.bias
-            rec["gain"] = self.gain
-            tpl = self._tpl = (arrays, at, np.array(rows, np.int64).reshape(-1, 6), rec)
+            tpl = self._tpl = (arrays, at, rows)
         return tpl
 
 
@@ -252,12 +248,13 @@ def pack_fields_into(fields, host, base):
         arrays = [a for t in tpls for a in t[0]]
         if arrays:
             np.concatenate(arrays, out=host[desc_doubles:total])
-        rows = [t[2] for t in tpls]
-        counts = np.fromiter((r.shape[0] for r in rows), np.int64, n)
-        out = np.array([t[3] for t in tpls], FIELD_DTYPE)
+        counts = np.fromiter((len(t[2]) for t in tpls), np.int64, n)
+        out = np.zeros(n, FIELD_DTYPE)
         out["tables"] = base + 8 * (8 * _TABLE_DOUBLES) * np.arange(n, dtype=np.uint64)
+        out["bias"] = np.stack([f.bias for f in fields])
+        out["gain"] = np.stack([f.gain for f in fields])
         if counts.sum():
-            r = np.concatenate(rows)
+            r = np.array([row for t in tpls for row in t[2]], np.int64)
             owner = np.repeat(np.arange(n), counts)
             tab = host[:desc_doubles].view(TABLE_DTYPE)
             slot = 8 * owner + r[:, 0]
