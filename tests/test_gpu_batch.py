@@ -280,3 +280,47 @@ def test_ragged_batch_edge_instances(cuda):
         assert np.array_equal(finals[0], np.zeros(2, complex))
         for k in range(1, len(specs)):
             assert np.array_equal(finals[k], b.result(k).state[-1])
+
+
+def test_full_uneven_tone_batch_properties(cuda):
+    """The full 1024-instance uneven tone batch (durations 10 us - 10 ms, 1.4e8 steps) at its real
+    size, through size-independent properties: every time grid is t0 + dt_out * i exactly, every
+    operator is unitary, every state has unit norm, the FP32-bulk final states are within 1e-6 of
+    the FP64 form's, and an instance sampled at random matches the oracle."""
+    import torch
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    rng = np.random.default_rng(3)
+    insts = []
+    for k in range(1024):
+        spin = ss.SpinQuantumNumber.HALF if rng.uniform() < 0.7 else ss.SpinQuantumNumber.ONE
+        dur = float(np.exp(rng.uniform(np.log(10e-6), np.log(10e-3))))
+        p = F.tone_parameters(np.random.default_rng(10_000 + k))
+        insts.append(B.Instance(spin, 0.0, dur, 10e-9, 1e-6, spin.plus_z if spin.dimension == 2 else spin.plus_x,
+                                sweep_parameters=p, field=tone_field(p)))
+    plans = {}
+    bulk = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+    plain = B.Batch(insts, precision=ss.Precision.FP64, plan_cache=plans)
+    assert bulk.total_steps > 1e8
+    bulk.run()
+    plain.run()
+    torch.cuda.synchronize()
+    for b, tol in ((plain, 1e-10), (bulk, 1e-6)):
+        worst_u = worst_norm = 0.0
+        for k, inst in enumerate(insts):
+            r = b.result(k)
+            n = r.time.shape[0]
+            assert np.array_equal(r.time, 0.0 + 1e-6 * np.arange(n))
+            u = r.time_evolution
+            d = u.shape[1]
+            eye = np.eye(d)
+            worst_u = max(worst_u, np.abs(np.einsum("nij,nkj->nik", u, u.conj()) - eye).max())
+            worst_norm = max(worst_norm, np.abs(np.linalg.norm(r.state, axis=1) - 1.0).max())
+        assert worst_u < tol and worst_norm < tol, (tol, worst_u, worst_norm)
+    fb, fp = bulk.final_states(), plain.final_states()
+    assert max(np.abs(a - c).max() for a, c in zip(fb, fp)) < 1e-6
+    for k in rng.choice(1024, 3, replace=False):
+        inst = insts[k]
+        d = inst.spin.dimension
+        t, u, s, sp = O.evaluate(d, O.Field(8), inst.sweep_parameters, 0.0, inst.time_end, 10e-9, 1e-6, inst.state_init)
+        assert np.abs(plain.result(int(k)).state - s).max() < 1e-10
