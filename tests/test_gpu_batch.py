@@ -324,3 +324,31 @@ def test_full_uneven_tone_batch_properties(cuda):
         d = inst.spin.dimension
         t, u, s, sp = O.evaluate(d, O.Field(8), inst.sweep_parameters, 0.0, inst.time_end, 10e-9, 1e-6, inst.state_init)
         assert np.abs(plain.result(int(k)).state - s).max() < 1e-10
+
+
+def test_fp32_bulk_uneven_tone_counts(cuda):
+    """Tone synthesis with channels of different tone counts: more tones than the per-channel
+    synthesis slots (the rest sampled directly), none, and a few with a bias; spin half and spin one,
+    against the FP64 form."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    rng = np.random.default_rng(21)
+
+    def tones(n):
+        return np.column_stack([ss.fields.TAU * rng.uniform(0, 1e6, n), rng.uniform(0, ss.fields.TAU * 10e3, n),
+                                rng.uniform(0, ss.fields.TAU, n)]) if n else None
+
+    insts = []
+    for k in range(12):
+        chans = {c: tones(n) for c, n in zip((0, 1, 2), (11, 0, 2)) if n}
+        f = ss.ToneField(chans, bias=[0.0, 3e3, ss.fields.TAU * 2e3])
+        spin = ss.SpinQuantumNumber.HALF if k % 2 else ss.SpinQuantumNumber.ONE
+        insts.append(B.Instance(spin, 0.0, float(rng.uniform(50e-6, 400e-6)), 10e-9, 1e-6, spin.plus_x, field=f))
+    plans = {}
+    bulk = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+    plain = B.Batch(insts, precision=ss.Precision.FP64, plan_cache=plans)
+    bulk.run()
+    plain.run()
+    for k in range(len(insts)):
+        assert np.abs(bulk.result(k).state - plain.result(k).state).max() < 1e-6, k
+        assert np.array_equal(bulk.result(k).time, plain.result(k).time)
