@@ -39,8 +39,12 @@ class Instance:
     intervals: Optional[tuple] = None
 
 
+INSTANCE_DTYPE = np.dtype(_lib.Instance)
+
+
 class Batch:
-    """A fixed list of instances prepared for repeated launches.
+    """A fixed list of instances (``Instance``, or any objects with its attributes) prepared for
+    repeated launches.
 
     Parameters mirror Simulator: ``get_field`` (a user function shared by all instances, or None for
     per-instance built-in fields), ``integration_method``, ``exponentiation_half`` /
@@ -137,7 +141,7 @@ class Batch:
         _lib.check(lib.spinsim_batch_describe(n, t0.ctypes.data, t1.ctypes.data, dti.ctypes.data, dto.ctypes.data,
                                               dims.ctypes.data, psi0.ctypes.data, insts, totals))
         out_off, u_off, st_off, self.total_steps = (int(v) for v in totals)
-        self._inst_np = np.frombuffer(insts, dtype=np.dtype(_lib.Instance))
+        self._inst_np = np.frombuffer(insts, dtype=INSTANCE_DTYPE)
         if any(getattr(i, "intervals", None) is not None for i in self.instances):
             out_off, u_off, st_off = self._restrict_to_pieces()
         keep = []
@@ -172,16 +176,11 @@ class Batch:
                 raise ValueError("memory() must return a 256-byte aligned uint8 tensor of the requested size")
         self.memory = buf
 
-        def piece(name, dtype):
-            o = offsets[name]
-            return buf[o:o + pieces[name]].view(dtype)
-
-        self.time = piece("time", torch.float64)
-        self.u = piece("u", torch.complex128)
-        self.state = piece("state", torch.complex128)
-        self.spin = piece("spin", torch.float64).view(-1, 3)
-        self.workspace = piece("workspace", torch.uint8)
-        field_dev = piece("fields", torch.float64)
+        # device addresses of the pieces; their tensor views are made on first use
+        self._pieces, self._offsets = pieces, offsets
+        base = buf.data_ptr()
+        self._ptr = {name: base + o for name, o in offsets.items()}
+        field_dev = self._piece("fields", torch.float64)
         # Field arrays and descriptors go through host memory: the caller's pinned staging buffer
         # when it is large enough (asynchronous copies: descriptors first, then fields), else
         # pageable memory (the copies wait for the stream).
@@ -214,11 +213,11 @@ class Batch:
         stream = torch.cuda.current_stream(dev).cuda_stream
         if staging is not None:
             _lib.check(lib.spinsim_batch_prepare_staged(self._plan, insts, n, fields_arr.ctypes.data, n,
-                                                        self.workspace.data_ptr(), ws_bytes, staging.data_ptr(),
+                                                        self._ptr["workspace"], ws_bytes, staging.data_ptr(),
                                                         desc_bytes, stream, ctypes.byref(handle)))
         else:
             _lib.check(lib.spinsim_batch_prepare(self._plan, insts, n, fields_arr.ctypes.data, n,
-                                                 self.workspace.data_ptr(), ws_bytes, stream, ctypes.byref(handle)))
+                                                 self._ptr["workspace"], ws_bytes, stream, ctypes.byref(handle)))
         # after the descriptor upload, so that torch's record of this copy on the pinned staging
         # block (which keeps the block from reuse until the copy is done) covers both
         field_dev.copy_(host_t, non_blocking=host_t.is_pinned())
@@ -231,9 +230,9 @@ class Batch:
         import torch
         if stream is None:
             stream = torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(self.lib.spinsim_batch_launch(self._handle, self.time.data_ptr(), self.u.data_ptr(),
-                                                 self.state.data_ptr() if with_state else None,
-                                                 self.spin.data_ptr() if (with_state and with_spin) else None, stream))
+        ptr = self._ptr
+        _lib.check(self.lib.spinsim_batch_launch(self._handle, ptr["time"], ptr["u"], ptr["state"] if with_state else None,
+                                                 ptr["spin"] if (with_state and with_spin) else None, stream))
 
     def capture(self):
         """Capture ``run`` into a CUDA graph; ``replay()`` then relaunches it."""
@@ -278,6 +277,49 @@ class Batch:
             rec[name][1:] = np.cumsum(per)[:-1]
         self.total_steps = int((n_out * rec["n_fine"]).sum())
         return int(n_out.sum()), int((2 * d * d * n_out).sum()), int((2 * d * n_out).sum())
+
+    def _piece(self, name, dtype):
+        o = self._offsets[name]
+        return self.memory[o:o + self._pieces[name]].view(dtype)
+
+    @property
+    def time(self):
+        """Output times of all instances, back to back (float64 device tensor)."""
+        if "_time" not in self.__dict__:
+            import torch
+            self._time = self._piece("time", torch.float64)
+        return self._time
+
+    @property
+    def u(self):
+        """Time-evolution operators of all instances, back to back (flat complex128 device tensor)."""
+        if "_u" not in self.__dict__:
+            import torch
+            self._u = self._piece("u", torch.complex128)
+        return self._u
+
+    @property
+    def state(self):
+        """States of all instances, back to back (flat complex128 device tensor)."""
+        if "_state" not in self.__dict__:
+            import torch
+            self._state = self._piece("state", torch.complex128)
+        return self._state
+
+    @property
+    def spin(self):
+        """Spin expectations of all instances, back to back ((sum N, 3) float64 device tensor)."""
+        if "_spin" not in self.__dict__:
+            import torch
+            self._spin = self._piece("spin", torch.float64).view(-1, 3)
+        return self._spin
+
+    @property
+    def workspace(self):
+        if "_workspace" not in self.__dict__:
+            import torch
+            self._workspace = self._piece("workspace", torch.uint8)
+        return self._workspace
 
     def layout_of(self, k):
         """(output offset, U offset, state offset (in doubles), N, d) of instance k."""

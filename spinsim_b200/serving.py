@@ -54,6 +54,9 @@ class Request:
     arrival: float = 0.0
     id: int = 0
     meta: dict = dc_field(default_factory=dict)
+    # a Request is also what a Batch reads as an instance (one evaluate() call, built-in field)
+    sweep_parameters = (0.0,)
+    intervals = None
 
     def instance(self):
         return Instance(self.spin, self.time_start, self.time_end, self.time_step_integration,
@@ -240,8 +243,7 @@ class Server:
 
         stream = self.streams[si]
         with torch.cuda.stream(stream):
-            b = Batch([r.instance() for r in reqs], plan_cache=self.plans, memory=memory, staging=self.staging[si],
-                      **self.kw)
+            b = Batch(reqs, plan_cache=self.plans, memory=memory, staging=self.staging[si], **self.kw)
             b.lease = lease[0]
             b.run()
             ev = torch.cuda.Event()
