@@ -198,3 +198,22 @@ def test_empty_and_single_step(cuda):
     assert r.time.shape == (0,) and r.state.shape == (0, 2) and r.spin.shape == (0, 3)
     r = sim.evaluate(0, 1e-6, 100e-9, 1e-6, ss.SpinQuantumNumber.HALF.plus_x, [1.0, 1.0])
     assert r.state.shape == (1, 2) and np.array_equal(r.state[0], ss.SpinQuantumNumber.HALF.plus_x)
+
+
+def test_gaussian_pi_pulse_known_answer(cuda):
+    """gaussian_example.py:22-26 on the device: a Gaussian pi pulse against its closed form (the
+    rotation angle is pi times the pulse's cumulative area; error below 1e-6 at dt = 0.01, the
+    reference documentation's figure) and against the oracle to 1e-10."""
+    import spinsim_b200 as ss
+
+    def cumulative(t):
+        return 0.5 * (1 + math.erf(t / math.sqrt(2.0))) - 0.5 * (1 + math.erf(-5.0 / math.sqrt(2.0)))
+
+    sim = ss.Simulator(F.gaussian_pulse, ss.SpinQuantumNumber.HALF)
+    res = sim.evaluate(-5.0, 7.0, 0.01, 2.0, [1.0, 0.0])
+    ana = np.array([[math.cos(0.5 * math.pi * cumulative(x)), -1j * math.sin(0.5 * math.pi * cumulative(x))]
+                    for x in res.time])
+    assert np.sqrt(np.sum(np.abs(res.state - ana) ** 2)) / 5 < 1e-6
+    t, u, s, sp = O.evaluate(2, O.Field(7), [0.0], -5.0, 7.0, 0.01, 2.0, [1.0, 0.0])
+    assert np.array_equal(res.time, t)
+    assert np.abs(res.state - s).max() < TOL
