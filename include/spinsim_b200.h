@@ -207,6 +207,18 @@ int spinsim_spin(int32_t dim, const double* state_dev, int64_t n_out, double* sp
  * the descriptors and the longest-first tile queue into the workspace (stream-ordered) and returns a
  * handle; launch issues only kernel launches and a counter reset, so it can be captured into a CUDA
  * graph and replayed.  Outputs are the flat arrays addressed by the instances' offsets. */
+/* Packs a batch's built-in fields (host only; no counterpart in the reference, whose samplers close
+ * over their own arrays, I:1941-2147) into one host buffer for one copy to the device buffer at
+ * device_base, and fills fields_out[n_fields] with device addresses.  Layout: eight table descriptors
+ * per tabulated field first, then every field's arrays (times shared between channels once).  plan:
+ * 8 int64 per row; per field a header {kind (1 tables, 2 tones), n_rows, bias (double[8]), gain
+ * (double[8], or 0 for ones), tone rows, tone row doubles, int32 tone_start[8] + tone_count[8], 0}
+ * followed, for tables, by n_rows channel rows {channel, time, amplitude, size, order, zero_boundary,
+ * alias (-1 or the field-local index of an earlier channel with the same times), 0}; the pointers are
+ * host addresses.  Returns the doubles written, or a negative error code. */
+int64_t spinsim_pack_fields(int32_t n_fields, const int64_t* plan, int64_t n_plan_rows, double* host,
+                            int64_t host_doubles, uint64_t device_base, spinsim_field* fields_out);
+
 /* Batch descriptors from evaluate() arguments (host only): for each instance i the step
  * normalisation of I:1025-1034 (as spinsim_normalise_steps), its output offsets packed one after
  * another in the flat arrays, field index i and psi0 from psi0[6 i .. 6 i + 2 dim) (re, im

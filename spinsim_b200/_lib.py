@@ -84,6 +84,7 @@ _SIGNATURES = [
     ("spinsim_batch_workspace_size", ctypes.c_size_t, [c_vp, ctypes.POINTER(Instance), c_i32, c_i32]),
     ("spinsim_batch_prepare", ctypes.c_int,
      [c_vp, ctypes.POINTER(Instance), c_i32, c_vp, c_i32, c_vp, ctypes.c_size_t, c_vp, ctypes.POINTER(c_vp)]),
+    ("spinsim_pack_fields", c_i64, [c_i32, c_vp, c_i64, c_vp, c_i64, ctypes.c_uint64, c_vp]),
     ("spinsim_spin_mean_workspace_size", ctypes.c_size_t, [c_i32, c_i64]),
     ("spinsim_spin_mean", ctypes.c_int, [c_vp, c_i64, c_i64, c_i32, c_i64, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     ("spinsim_piece_product", ctypes.c_int, [c_i32, c_vp, c_i64, c_vp, c_vp, ctypes.c_size_t, c_vp]),

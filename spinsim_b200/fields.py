@@ -103,27 +103,27 @@ class TabulatedField(BuiltinField):
     def packed_doubles(self):
         """float64 entries in a packed field buffer: eight 4-double table descriptors, then the
         times (once per distinct time array) and amplitudes."""
-        return 8 * _TABLE_DOUBLES + self._template()[1]
+        return 8 * _TABLE_DOUBLES + self._cplan()[1]
 
-    def _template(self):
-        """The field's part of a packed buffer, computed once (tables are snapshots): (arrays in
-        order, their total entries, rows (channel, time offset, amplitude offset, size, order,
-        zero_boundary) with offsets from the field's first array)."""
-        tpl = self.__dict__.get("_tpl")
-        if tpl is None:
-            arrays, rows, at, seen = [], [], 0, {}
-            for c in sorted(self.tables):
+    def _cplan(self):
+        """The field's rows of a ``spinsim_pack_fields`` plan (host pointers into the field's own
+        arrays, which are snapshots) and the doubles of its arrays; computed once."""
+        got = self.__dict__.get("_plan")
+        if got is None:
+            rows, index, n = [], {}, 0
+            for k, c in enumerate(sorted(self.tables)):
                 t, a, o, z = self.tables[c]
-                ti = seen.get(id(t))
-                if ti is None:
-                    ti = seen[id(t)] = at
-                    arrays.append(t)
-                    at += t.size
-                arrays.append(a)
-                rows.append((c, ti, at, t.size, o, int(z)))
-                at += a.size
-            tpl = self._tpl = (arrays, at, rows)
-        return tpl
+                alias = index.get(id(t), -1)
+                if alias < 0:
+                    index[id(t)] = k
+                    n += t.size
+                n += a.size
+                rows.append((c, t.ctypes.data, a.ctypes.data, t.size, o, int(z), alias, 0))
+            header = (1, len(rows), self.bias.ctypes.data, self.gain.ctypes.data, 0, 0, 0, 0)
+            # the arrays the pointers refer to stay referenced by the plan
+            keep = (self.bias, self.gain, [v[:2] for v in self.tables.values()])
+            got = self._plan = (np.array([header] + rows, np.int64), n, keep)
+        return got
 
 
 class ToneField(BuiltinField):
@@ -182,20 +182,18 @@ class ToneField(BuiltinField):
         return c in self.tones or self.bias[c] != 0.0
 
     def packed_doubles(self):
-        """float64 entries in a packed field buffer: the (w, A, phi) rows padded to 32 bytes."""
-        return (self.packed()[0].size + 3) // 4 * 4 or 4
+        """float64 entries in a packed field buffer: the (w, A, phi) rows."""
+        return self.packed()[0].size
 
-    def field_record(self):
-        """The field's spinsim_field struct without its tone pointer (computed once)."""
-        if "_record" not in self.__dict__:
-            rec = np.zeros((), FIELD_DTYPE)
-            _, start, count = self.packed()
-            rec["tone_start"] = start
-            rec["tone_count"] = count
-            rec["bias"] = self.bias
-            rec["gain"] = 1.0
-            self._record = rec
-        return self._record
+    def _cplan(self):
+        """The field's header row of a ``spinsim_pack_fields`` plan (computed once)."""
+        got = self.__dict__.get("_plan")
+        if got is None:
+            flat, start, count = self.packed()
+            self._counts = np.concatenate([start, count]).astype(np.int32)
+            header = (2, 0, self.bias.ctypes.data, 0, flat.ctypes.data, flat.size, self._counts.ctypes.data, 0)
+            got = self._plan = (np.array([header], np.int64), flat.size, (self.bias, flat, self._counts))
+        return got
 
     def sample(self, t):
         """Host evaluation (for plots and checks): array of shape (len(t), 8)."""
@@ -226,53 +224,23 @@ def packed_doubles(fields):
 
 
 def pack_fields_into(fields, host, base):
-    """Write the fields' arrays (and table descriptors) into ``host`` (a float64 array of at least
-    ``packed_doubles(fields)`` entries) for a device copy of ``host`` at address ``base`` (8-byte
-    aligned; the kernels read these arrays one double at a time); returns the ``spinsim_field``
-    structs as a numpy array of ``FIELD_DTYPE``.  Tabulated fields: all descriptors first, then every
-    field's arrays back to back."""
+    """Write the fields' arrays and table descriptors into ``host`` (a contiguous float64 array of
+    at least ``packed_doubles(fields)`` entries) for a device copy of ``host`` at address ``base``;
+    returns the ``spinsim_field`` structs as a numpy array of ``FIELD_DTYPE``.  Layout (the library's
+    ``spinsim_pack_fields``): the tabulated fields' descriptors first, then every field's arrays."""
     _check_fields(fields)
     n = len(fields)
+    out = np.zeros(n, FIELD_DTYPE)
     if not n:
-        return np.zeros(0, FIELD_DTYPE)
-    if isinstance(fields[0], TabulatedField):
-        tpls = [f._template() for f in fields]
-        desc_doubles = 8 * _TABLE_DOUBLES * n
-        sizes = np.fromiter((t[1] for t in tpls), np.int64, n)
-        first = np.empty(n, np.int64)
-        first[0] = desc_doubles
-        np.cumsum(sizes[:-1], out=first[1:])
-        first[1:] += desc_doubles
-        total = desc_doubles + int(sizes.sum())
-        host[:desc_doubles] = 0.0
-        arrays = [a for t in tpls for a in t[0]]
-        if arrays:
-            np.concatenate(arrays, out=host[desc_doubles:total])
-        counts = np.fromiter((len(t[2]) for t in tpls), np.int64, n)
-        out = np.zeros(n, FIELD_DTYPE)
-        out["tables"] = base + 8 * (8 * _TABLE_DOUBLES) * np.arange(n, dtype=np.uint64)
-        out["bias"] = np.stack([f.bias for f in fields])
-        out["gain"] = np.stack([f.gain for f in fields])
-        if counts.sum():
-            r = np.array([row for t in tpls for row in t[2]], np.int64)
-            owner = np.repeat(np.arange(n), counts)
-            tab = host[:desc_doubles].view(TABLE_DTYPE)
-            slot = 8 * owner + r[:, 0]
-            tab["time"][slot] = base + 8 * (first[owner] + r[:, 1]).astype(np.uint64)
-            tab["amplitude"][slot] = base + 8 * (first[owner] + r[:, 2]).astype(np.uint64)
-            tab["size"][slot] = r[:, 3]
-            tab["order"][slot] = r[:, 4]
-            tab["zero_boundary"][slot] = r[:, 5]
         return out
-    at = 0
-    starts = []
-    for f in fields:
-        flat = f.packed()[0]
-        host[at:at + flat.size] = flat
-        starts.append(at)
-        at += f.packed_doubles()
-    out = np.array([f.field_record() for f in fields], FIELD_DTYPE)
-    out["tones"] = base + 8 * np.array(starts, np.uint64)
+    if host.dtype != np.float64 or not host.flags["C_CONTIGUOUS"]:
+        raise ValueError("host must be a contiguous float64 array")
+    plan = np.concatenate([f._cplan()[0] for f in fields]) if n > 1 else fields[0]._cplan()[0]
+    lib = _lib.load()
+    used = lib.spinsim_pack_fields(n, plan.ctypes.data, plan.shape[0], host.ctypes.data, host.size, int(base),
+                                   out.ctypes.data)
+    if used < 0:
+        _lib.check(int(used))
     return out
 
 
