@@ -244,21 +244,6 @@ def pack_fields_into(fields, host, base):
     return out
 
 
-def pack_fields(fields, device):
-    """Device structs for a list of built-in fields with one host-to-device copy.
-
-    All tone arrays, table arrays and table descriptors go into one float64 buffer; returns
-    (numpy array of spinsim_field structs, [device buffer], host bytes copied)."""
-    import torch
-    fields = list(fields)
-    total = max(4, packed_doubles(fields))
-    dev = torch.empty(total, dtype=torch.float64, device=device)
-    host = np.zeros(total)
-    structs = pack_fields_into(fields, host, dev.data_ptr())
-    dev.copy_(torch.from_numpy(host))
-    return structs, [dev], host.nbytes
-
-
 # ---------------------------------------------------------------------------- sampler factory
 def _sampler_body(time, amplitude, order, zero_boundary):
     """Python source-level sampler (compiled by numba for CUDA or CPU).  Restates the reference's
