@@ -444,7 +444,7 @@ class Evaluator:
         keep, outs, self.h2d_bytes, self.d2h_bytes = [], [], 0, 0
         for a, b in self.groups(instances):
             stream = self.compute
-            with torch.cuda.stream(stream):
+            with torch.cuda.stream(stream), torch.cuda.nvtx.range(f"spinsim.evaluate.group[{a}:{b}]"):
                 batch = Batch(instances[a:b], plan_cache=self.plans, staging=self._pinned, **self.kw)
                 batch.run()
                 done = torch.cuda.Event()

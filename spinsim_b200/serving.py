@@ -242,7 +242,7 @@ class Server:
             return self.arena.buffer[blk[0]:blk[0] + blk[1]]
 
         stream = self.streams[si]
-        with torch.cuda.stream(stream):
+        with torch.cuda.stream(stream), torch.cuda.nvtx.range(f"spinsim.serve.launch[{len(reqs)}]"):
             b = Batch(reqs, plan_cache=self.plans, memory=memory, staging=self.staging[si], **self.kw)
             b.lease = lease[0]
             b.run()

@@ -217,3 +217,20 @@ def test_gaussian_pi_pulse_known_answer(cuda):
     t, u, s, sp = O.evaluate(2, O.Field(7), [0.0], -5.0, 7.0, 0.01, 2.0, [1.0, 0.0])
     assert np.array_equal(res.time, t)
     assert np.abs(res.state - s).max() < TOL
+
+
+@pytest.mark.parametrize("spin_name", ["HALF", "ONE"])
+def test_rabi_rotating_wave_limit(cuda, spin_name):
+    """example.py:33-45's dressed Rabi drive in the rotating-wave limit (drive 2 kHz, bias 1 MHz):
+    the spin's z component follows cos(Omega t) (times 1/2 for spin half) to the size of the
+    counter-rotating corrections, Omega / omega = 2e-3."""
+    import spinsim_b200 as ss
+    spin = getattr(ss.SpinQuantumNumber, spin_name)
+    omega, rabi = math.tau * 1e6, math.tau * 2e3
+    field = F.rabi if spin == ss.SpinQuantumNumber.HALF else F.rabi_one
+    sim = ss.Simulator(field, spin)
+    res = sim.evaluate(0.0, 1e-3, 10e-9, 1e-6, spin.plus_z, [omega, rabi])
+    scale = 0.5 if spin == ss.SpinQuantumNumber.HALF else 1.0
+    z = res.spin[:, 2] / scale
+    assert np.abs(z - np.cos(rabi * res.time)).max() < 1e-2
+    assert np.abs(np.linalg.norm(res.state, axis=1) - 1.0).max() < 1e-10
