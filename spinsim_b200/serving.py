@@ -309,16 +309,21 @@ class Server:
         self._thread.start()
         return self
 
-    def submit(self, request):
+    def submit(self, request, timeout=None):
         """Queue ``request`` (a ``Request``; its arrival is now) and return a
         ``concurrent.futures.Future`` that resolves to its ``Results`` (views of the arena, which the
-        request's block holds until they are released) or to the launch's exception."""
+        request's block holds until they are released) or to the launch's exception.  With
+        ``timeout`` (seconds), a request not yet admitted to a launch by then fails with
+        ``TimeoutError`` (checked when it reaches the head of the queue); cancelling the future
+        before admission withdraws the request."""
         if getattr(self, "_thread", None) is None or self._stopping.is_set():
             raise RuntimeError("the server is not running: call start()")
         if request.footprint() > self.arena.size:
             raise ValueError(f"request {request.id} needs {request.footprint()} bytes, above the HBM budget")
         future = concurrent.futures.Future()
         request.arrival = time.perf_counter() - self._t0
+        if timeout is not None:
+            request.meta["deadline"] = request.arrival + float(timeout)
         self._inbox.put((request, future))
         return future
 
@@ -364,6 +369,12 @@ class Server:
                         futures[id(req)] = fut
                         queue.append(req)
                 inflight = self._complete(inflight, free_streams, [], clock, t0, resolve, False)
+                now = clock() - t0
+                while queue and queue[0].meta.get("deadline", math.inf) < now:
+                    r = queue.popleft()
+                    futures.pop(id(r)).set_exception(
+                        TimeoutError(f"request {r.id} was not admitted within its timeout"))
+                    self.stats["timeouts"] += 1
                 while queue and free_streams:
                     try:
                         if not self._admit(queue, inflight, free_streams, clock, t0):

@@ -120,3 +120,17 @@ def test_async_submit_futures(cuda):
         assert np.array_equal(res.time_evolution, sync[r.id].time_evolution)
     with pytest.raises(RuntimeError):
         srv.submit(reqs[0])  # closed
+
+
+def test_async_timeout_and_cancel(cuda):
+    """A request whose timeout passes before admission fails with TimeoutError; others still run."""
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Server
+    reqs = requests(n=6, rate=1e5, seed=23)
+    with Server(precision=ss.Precision.FP64, streams=2) as srv:
+        late = srv.submit(reqs[0], timeout=-1.0)  # already past its deadline
+        ok = [srv.submit(r) for r in reqs[1:]]
+        with pytest.raises(TimeoutError):
+            late.result(timeout=60)
+        assert all(f.result(timeout=120) is not None for f in ok)
+        assert srv.stats["timeouts"] == 1
