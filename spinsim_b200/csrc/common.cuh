@@ -106,10 +106,12 @@ struct EvolveArgs {
 constexpr int kBulkTones = 8;               // tones per channel (x, y, z) synthesised per warp
 constexpr int kToneSlots = 3 * kBulkTones;  // slot = channel * kBulkTones + tone
 constexpr int kSynthIntervals = 2;          // output intervals per lane, 32 intervals apart
+// Slot-fastest layouts: a warp's 16-byte stores and loads of one quantity for all slots are
+// contiguous (no bank conflicts); the consumers' reads of one slot are broadcasts.
 struct ToneShared {
-    double l[kToneSlots][32][2];                    // [slot][lane] (re, im) of L for the lane's first interval
-    double uv[2][kToneSlots][kSynthIntervals][4];   // [buffer][slot][interval] G^i U, G^i V of the step
-    double rg[kToneSlots][6];                       // [slot] exp(i w dt), exp(i w (a_hi - a_lo)), G
+    double l[kToneSlots][32][2];                 // [slot][lane] (re, im) of L for the lane's first interval
+    double2 uv[2][kSynthIntervals][2][kToneSlots];  // [buffer][interval][U or V][slot] G^i U, G^i V of the step
+    double2 rg[3][kToneSlots];                   // [exp(i w dt), exp(i w (a_hi - a_lo)), G][slot]
 };
 constexpr int kToneSharedBytes =
     kToneSlots * 32 * 2 * 8 + 2 * kToneSlots * kSynthIntervals * 4 * 8 + kToneSlots * 6 * 8;

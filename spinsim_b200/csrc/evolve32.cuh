@@ -459,7 +459,7 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
             sincos(w * (__dmul_rn(dt_out, (double)(i0 + 32)) - __dmul_rn(dt_out, (double)i0)), &rg[5], &rg[4]);
         }
 #pragma unroll
-        for (int q = 0; q < 6; q++) ts->rg[lane][q] = rg[q];
+        for (int q = 0; q < 3; q++) ts->rg[q][lane] = make_double2(rg[2 * q], rg[2 * q + 1]);
     }
 
     Su2d su2[NI];
@@ -468,16 +468,13 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
     for (int j = 0; j < K; j++) {
         // publish G^i U, G^i V of step j
         if (lane < kToneSlots) {
-            const double* rg = ts->rg[lane];
-            const c64 rot = c64{rg[0], rg[1]}, gap = c64{rg[2], rg[3]}, g = c64{rg[4], rg[5]};
+            const double2 r0 = ts->rg[0][lane], r1 = ts->rg[1][lane], r2 = ts->rg[2][lane];
+            const c64 rot = c64{r0.x, r0.y}, gap = c64{r1.x, r1.y}, g = c64{r2.x, r2.y};
             c64 uu = u_prod, vv = u_prod * gap;
 #pragma unroll
             for (int i = 0; i < NI; i++) {
-                double* dst = ts->uv[j & 1][lane][i];
-                dst[0] = uu.re;
-                dst[1] = uu.im;
-                dst[2] = vv.re;
-                dst[3] = vv.im;
+                ts->uv[j & 1][i][0][lane] = make_double2(uu.re, uu.im);
+                ts->uv[j & 1][i][1][lane] = make_double2(vv.re, vv.im);
                 if (i + 1 < NI) {
                     uu = uu * g;
                     vv = vv * g;
@@ -504,8 +501,8 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
                 const double2 lv = *reinterpret_cast<const double2*>(ts->l[slot][lane]);
 #pragma unroll
                 for (int i = 0; i < NI; i++) {
-                    const double2 uu = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][i][0]);
-                    const double2 vv = *reinterpret_cast<const double2*>(&ts->uv[j & 1][slot][i][2]);
+                    const double2 uu = ts->uv[j & 1][i][0][slot];
+                    const double2 vv = ts->uv[j & 1][i][1][slot];
                     if (k & 1) {
                         pa[i] = fma(lv.x, uu.y, fma(lv.y, uu.x, pa[i]));
                         pb[i] = fma(lv.x, vv.y, fma(lv.y, vv.x, pb[i]));
