@@ -111,10 +111,8 @@ constexpr int kSynthIntervals = 2;          // output intervals per lane, 32 int
 struct ToneShared {
     double l[kToneSlots][32][2];                 // [slot][lane] (re, im) of L for the lane's first interval
     double2 uv[2][kSynthIntervals][2][kToneSlots];  // [buffer][interval][U or V][slot] G^i U, G^i V of the step
-    double2 rg[3][kToneSlots];                   // [exp(i w dt), exp(i w (a_hi - a_lo)), G][slot]
 };
-constexpr int kToneSharedBytes =
-    kToneSlots * 32 * 2 * 8 + 2 * kToneSlots * kSynthIntervals * 4 * 8 + kToneSlots * 6 * 8;
+constexpr int kToneSharedBytes = kToneSlots * 32 * 2 * 8 + 2 * kToneSlots * kSynthIntervals * 4 * 8;
 
 // ------------------------------------------------------------------ complex helpers (FP64)
 struct c64 {

@@ -445,21 +445,19 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
         ts->l[slot][lane][0] = re;
         ts->l[slot][lane][1] = im;
     }
-    c64 u_prod = c64{0.0, 0.0};
+    // producer constants of slot `lane` (registers for the whole tile): exp(i w dt), exp(i w (a_hi - a_lo)), G
+    c64 u_prod = c64{0.0, 0.0}, rot = c64{1.0, 0.0}, gap = c64{1.0, 0.0}, g = c64{1.0, 0.0};
     if (lane < kToneSlots) {
         const int c = lane / kBulkTones, k = lane % kBulkTones;
-        double rg[6] = {1.0, 0.0, 1.0, 0.0, 1.0, 0.0};
         if (k < f.tone_count[c]) {
             const double w = __ldg(f.tones + 3 * (f.tone_start[c] + k));
             sincos(w * a_lo, &u_prod.im, &u_prod.re);
-            sincos(w * dt, &rg[1], &rg[0]);
-            sincos(w * (a_hi - a_lo), &rg[3], &rg[2]);
+            sincos(w * dt, &rot.im, &rot.re);
+            sincos(w * (a_hi - a_lo), &gap.im, &gap.re);
             // G = exp(i w (t_c(l + 32) - t_c(l))), t_c rounded as the intervals' own starts are
             const int64_t i0 = inst.interval0 + index[0];
-            sincos(w * (__dmul_rn(dt_out, (double)(i0 + 32)) - __dmul_rn(dt_out, (double)i0)), &rg[5], &rg[4]);
+            sincos(w * (__dmul_rn(dt_out, (double)(i0 + 32)) - __dmul_rn(dt_out, (double)i0)), &g.im, &g.re);
         }
-#pragma unroll
-        for (int q = 0; q < 3; q++) ts->rg[q][lane] = make_double2(rg[2 * q], rg[2 * q + 1]);
     }
 
     Su2d su2[NI];
@@ -468,8 +466,6 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
     for (int j = 0; j < K; j++) {
         // publish G^i U, G^i V of step j
         if (lane < kToneSlots) {
-            const double2 r0 = ts->rg[0][lane], r1 = ts->rg[1][lane], r2 = ts->rg[2][lane];
-            const c64 rot = c64{r0.x, r0.y}, gap = c64{r1.x, r1.y}, g = c64{r2.x, r2.y};
             c64 uu = u_prod, vv = u_prod * gap;
 #pragma unroll
             for (int i = 0; i < NI; i++) {
