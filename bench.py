@@ -85,7 +85,7 @@ FLOPS_BULK = {2: {"fp64": 290, "fp32": 90}, 3: {"fp64": 296, "fp32": 90}}
 # DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload
 # (max_registers 168, state scan not run), from one capture of
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve -c 1`.
-TRAFFIC_BYTES_PER_LAUNCH = 1684480 + 81413888
+TRAFFIC_BYTES_PER_LAUNCH = 1834240 + 81415168
 
 
 def algorithmic_bytes(specs):
