@@ -577,7 +577,8 @@ def main():
         return
     import torch
     if not torch.cuda.is_available():
-        print(json.dumps({"metric": METRIC, "unavailable": "no CUDA device"}))
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "unavailable": "no CUDA device"}))
         return
     torch.cuda.set_device(local)
     if args.workload == "serving":
