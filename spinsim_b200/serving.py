@@ -122,7 +122,13 @@ class Completed:
 
 
 class Arena:
-    """One device allocation handed out in 256-byte aligned blocks (first fit, coalescing frees)."""
+    """One device allocation handed out in 256-byte aligned blocks (first fit, coalescing frees).
+
+    ``take`` and ``largest_free`` may be called from several threads; ``give`` may be called from
+    any thread at any time, including from a finalizer that runs while another thread is inside
+    ``take`` (a client dropping its ``Results`` while the serving thread admits a launch).  So
+    ``give`` only queues the block on a lock-free ``SimpleQueue``, and the free list is changed
+    only under the lock, where the queued blocks are merged back first."""
 
     ALIGN = 256
 
@@ -132,30 +138,54 @@ class Arena:
         self.buffer = torch.empty(self.size, dtype=torch.uint8, device=device)
         self._starts = [0]          # free blocks, sorted by offset
         self._sizes = {0: self.size}
-        self.in_use = 0
+        self._returned = queue_mod.SimpleQueue()  # blocks given back, not yet merged
+        self._lock = threading.Lock()
+        self._in_use = 0
+
+    @property
+    def in_use(self):
+        """Bytes handed out and not yet given back."""
+        with self._lock:
+            self._merge_returned()
+            return self._in_use
 
     def largest_free(self):
-        return max(self._sizes.values(), default=0)
+        with self._lock:
+            self._merge_returned()
+            return max(self._sizes.values(), default=0)
 
     def take(self, nbytes):
         """Offset of a free block of ``nbytes`` (rounded up to the alignment), or None."""
         n = (int(nbytes) + self.ALIGN - 1) // self.ALIGN * self.ALIGN
-        for i, off in enumerate(self._starts):
-            size = self._sizes[off]
-            if size >= n:
-                del self._sizes[off]
-                if size == n:
-                    del self._starts[i]
-                else:
-                    self._starts[i] = off + n
-                    self._sizes[off + n] = size - n
-                self.in_use += n
-                return off, n
+        with self._lock:
+            self._merge_returned()
+            for i, off in enumerate(self._starts):
+                size = self._sizes[off]
+                if size >= n:
+                    del self._sizes[off]
+                    if size == n:
+                        del self._starts[i]
+                    else:
+                        self._starts[i] = off + n
+                        self._sizes[off + n] = size - n
+                    self._in_use += n
+                    return off, n
         return None
 
     def give(self, off, n):
-        """Return the block [off, off + n) (from ``take``)."""
-        self.in_use -= n
+        """Return the block [off, off + n) (from ``take``); safe from any thread or finalizer."""
+        self._returned.put((off, n))
+
+    def _merge_returned(self):
+        while True:
+            try:
+                off, n = self._returned.get_nowait()
+            except queue_mod.Empty:
+                return
+            self._insert(off, n)
+
+    def _insert(self, off, n):
+        self._in_use -= n
         i = bisect.bisect_left(self._starts, off)
         if i < len(self._starts) and off + n == self._starts[i]:  # merge with the next block
             nxt = self._starts.pop(i)
@@ -165,6 +195,12 @@ class Arena:
         else:
             self._starts.insert(i, off)
             self._sizes[off] = n
+
+    def free_blocks(self):
+        """The free list as sorted (offset, size) pairs, after merging returned blocks."""
+        with self._lock:
+            self._merge_returned()
+            return [(o, self._sizes[o]) for o in self._starts]
 
 
 class _Lease:
@@ -242,14 +278,20 @@ class Server:
             return self.arena.buffer[blk[0]:blk[0] + blk[1]]
 
         stream = self.streams[si]
-        with torch.cuda.stream(stream), torch.cuda.nvtx.range(f"spinsim.serve.launch[{len(reqs)}]"):
-            b = Batch(reqs, plan_cache=self.plans, memory=memory, staging=self.staging[si], **self.kw)
-            b.lease = lease[0]
-            b.run()
-            ev = torch.cuda.Event()
-            if self.copy_to_host:
-                b.host = [t.to("cpu", non_blocking=True) for t in (b.time, b.u, b.state, b.spin)]
-            ev.record(stream)
+        try:
+            with torch.cuda.stream(stream), torch.cuda.nvtx.range(f"spinsim.serve.launch[{len(reqs)}]"):
+                b = Batch(reqs, plan_cache=self.plans, memory=memory, staging=self.staging[si], **self.kw)
+                b.lease = lease[0]
+                b.run()
+                ev = torch.cuda.Event()
+                if self.copy_to_host:
+                    b.host = [t.to("cpu", non_blocking=True) for t in (b.time, b.u, b.state, b.spin)]
+                ev.record(stream)
+        except BaseException:
+            # uploads or kernels already queued on the stream may still write into the block: let
+            # them finish before the lease (and with it the block and the stream) can be reused
+            stream.synchronize()
+            raise
         return b, ev, lease[0]
 
     def run(self, requests, clock=time.perf_counter, idle_sleep=20e-6, on_complete=None, keep_results=True):

@@ -1,13 +1,14 @@
 """Generate the golden fixtures in ``tests/golden/golden.npz`` by running the reference itself.
 
-The reference (alexander-tritt-monash/spinsim, one Python file on numba) is imported from
-``/root/reference`` with a stub ``numba.roc`` module: the reference's top-level ``from numba import
-roc`` (spinsim/__init__.py:8) is the only thing that fails on the numba in this image, and the ROC
-branches are dead code on the CPU device.  Every case runs ``Simulator(..., device=Device.CPU)``
+The reference (alexander-tritt-monash/spinsim, one Python file on numba) is imported from the
+directory given by ``--reference`` (or the ``SPINSIM_REFERENCE`` environment variable) with a stub
+``numba.roc`` module: the reference's top-level ``from numba import roc`` (spinsim/__init__.py:8)
+is the only thing that fails on the numba in this image, and the ROC branches are dead code on the
+CPU device.  Every case runs ``Simulator(..., device=Device.CPU)``
 (spinsim/__init__.py:375, :993) and stores ``time``, ``time_evolution``, ``state`` and ``spin``.
 
-Usage: ``python tests/golden/make_golden.py [--reference /root/reference]``.  Only this script reads
-the reference; the tests read the committed ``golden.npz``.
+Usage: ``python tests/golden/make_golden.py --reference <path to the reference checkout>``.  Only this
+script reads the reference; the tests read the committed ``golden.npz``.
 """
 import argparse
 import json
@@ -135,9 +136,12 @@ def make_table_field(spinsim, tables, order, zero_boundary, spin):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("SPINSIM_REFERENCE"),
+                    help="directory holding the reference's spinsim/ package (or set SPINSIM_REFERENCE)")
     ap.add_argument("--out", default=os.path.join(HERE, "golden.npz"))
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set SPINSIM_REFERENCE")
     spinsim = import_reference(args.reference)
     cases, tables = build_cases()
     spins = {"half": spinsim.SpinQuantumNumber.HALF, "one": spinsim.SpinQuantumNumber.ONE}

@@ -134,3 +134,44 @@ def test_async_timeout_and_cancel(cuda):
             late.result(timeout=60)
         assert all(f.result(timeout=120) is not None for f in ok)
         assert srv.stats["timeouts"] == 1
+
+
+def test_async_results_dropped_on_client_thread_while_admitting(cuda):
+    """Clients drop their Results (the arena block's finalizer runs on the client thread) while the
+    serving thread admits further launches into the same arena: every result still matches the
+    synchronous run and the arena is whole again at the end."""
+    import gc
+    import queue
+    import threading
+    import spinsim_b200 as ss
+    from spinsim_b200.serving import Server
+    reqs = requests(n=40, rate=1e5, seed=31)
+    sync = {c.request.id: c.results.state.copy() for c in Server(precision=ss.Precision.FP64, streams=2).run(reqs)}
+    mismatches = []
+    srv = Server(precision=ss.Precision.FP64, streams=4, max_batch=3,
+                 hbm_budget=2 * sum(r.footprint() for r in reqs) + (1 << 20))
+    work = queue.Queue()
+    with srv:
+        for r in reqs:
+            work.put((r, srv.submit(r)))
+
+        def client():
+            while True:
+                try:
+                    r, f = work.get_nowait()
+                except queue.Empty:
+                    return
+                res = f.result(timeout=120)
+                if not np.array_equal(res.state, sync[r.id]):
+                    mismatches.append(r.id)
+                del res, f  # the launch's block returns to the arena from this thread
+
+        threads = [threading.Thread(target=client) for _ in range(3)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+    gc.collect()
+    assert not mismatches
+    assert srv.arena.in_use == 0
+    assert srv.arena.free_blocks() == [(0, srv.arena.size)]

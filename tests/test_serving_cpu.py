@@ -41,7 +41,7 @@ def test_arena_coalesces_in_any_order():
             a.give(*blocks[k])
         assert a.in_use == 0
         assert a.largest_free() == a.size
-        assert a._starts == [0]
+        assert a.free_blocks() == [(0, a.size)]
 
 
 def test_arena_reuses_freed_hole():
@@ -93,3 +93,56 @@ def test_pulse_sequence_is_zero_order_hold_on_x_or_y():
     assert not np.any((ax != 0) & (ay != 0))  # one axis at a time
     widths = np.diff(tx)[on[:-1]]
     assert np.all(np.isclose(widths, 10e-6) | np.isclose(widths, 20e-6))
+
+
+def test_arena_gives_from_other_threads_while_taking():
+    """Blocks given back from other threads (a client dropping Results: the lease's finalizer runs
+    on the client thread) while one thread takes blocks: no block is handed out twice and the free
+    list coalesces back to one block."""
+    import threading
+    import queue
+    from spinsim_b200.serving import _Lease
+    a = arena(1 << 20)
+    handoff = queue.Queue()
+    stop = threading.Event()
+    errors = []
+
+    def client():
+        while not stop.is_set() or not handoff.empty():
+            try:
+                lease = handoff.get(timeout=0.01)
+            except queue.Empty:
+                continue
+            del lease  # the finalizer gives the block back on this thread
+
+    clients = [threading.Thread(target=client) for _ in range(3)]
+    for t in clients:
+        t.start()
+    rng = np.random.default_rng(5)
+    live = {}
+    try:
+        for it in range(4000):
+            blk = a.take(int(rng.integers(1, 20_000)))
+            if blk is None:
+                continue
+            off, n = blk
+            for o, m in live.items():  # no overlap with blocks still held here
+                if off < o + m and o < off + n:
+                    errors.append((blk, (o, m)))
+            if rng.uniform() < 0.5:
+                live[off] = n
+            else:
+                handoff.put(_Lease(a, off, n))
+            if len(live) > 20:
+                o = next(iter(live))
+                handoff.put(_Lease(a, o, live.pop(o)))
+    finally:
+        stop.set()
+        for t in clients:
+            t.join()
+    for o, m in live.items():
+        a.give(o, m)
+    gc.collect()
+    assert not errors
+    assert a.in_use == 0
+    assert a.free_blocks() == [(0, a.size)]
