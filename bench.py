@@ -542,7 +542,8 @@ def profile_case(args):
     if args.profile_size == "small":
         specs = [(d, min(t, 1e-3), p) for d, t, p in specs[:256]]
     prec = ss.Precision.FP32_BULK if args.precision == "fp32_bulk" else ss.Precision.FP64
-    b = Batch(instances(ss, specs), precision=prec, max_registers=args.max_registers, lanes=args.lanes)
+    b = Batch(instances(ss, specs), precision=prec, max_registers=args.max_registers, lanes=args.lanes,
+              variant=args.variant)
     b.run(with_state=not args.evolve_only)
     torch.cuda.synchronize()
     return {"workload": f"profile-{args.profile_size}", "precision": args.precision, "steps": b.total_steps,
@@ -561,6 +562,7 @@ def main():
     ap.add_argument("--precision", default="fp32_bulk", choices=["fp32_bulk", "fp64"])
     ap.add_argument("--max-registers", type=int, default=168)
     ap.add_argument("--lanes", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=0, help="FP32-bulk tone kernel: 0 tensor path, 1 warp synthesis")
     ap.add_argument("--evolve-only", action="store_true")
     ap.add_argument("--e2e-chunks", type=int, default=6, help="groups overlapped in the end-to-end measurement")
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")

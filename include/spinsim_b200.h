@@ -46,6 +46,11 @@ extern "C" {
 #define SPINSIM_FIELD_TONES 2 /* per-channel bias + sum of sinusoids */
 #define SPINSIM_PRECISION_FP64 0
 #define SPINSIM_PRECISION_FP32_BULK 1
+/* Kernel of FP32-bulk plans with tone fields (spinsim_plan_desc.variant): the field samples of a
+ * tile of output intervals as FP64 tensor-core matrix products (the default), or a warp-synchronous
+ * phasor synthesis. */
+#define SPINSIM_VARIANT_TENSOR 0
+#define SPINSIM_VARIANT_SYNTH 1
 
 /* Plan description: the compile-time specialisation of the reference's compile_time_evolver
  * (I:453-991), i.e. Simulator.__init__ (I:375) minus the user callable. */
@@ -62,7 +67,7 @@ typedef struct {
     int32_t max_registers;     /* 0 = no cap; <= 128 selects the 128-register build (built-in fields)
                                   or is passed to the JIT linker (user fields) */
     int32_t lanes;             /* lanes per output interval: 0 = auto, else 1, 2, 4, 8, 16 or 32 */
-    int32_t reserved;
+    int32_t variant;           /* SPINSIM_VARIANT_* (FP32-bulk tone plans; ignored otherwise) */
 } spinsim_plan_desc;
 
 /* One interpolation table: generate_interpolation_sampler's (time, amplitude, order,
@@ -121,6 +126,8 @@ typedef struct {
     int32_t sm_count;
     int32_t lanes;
     int32_t linked;         /* 1 if the kernel came from nvJitLink (user field) */
+    int32_t variant;        /* SPINSIM_VARIANT_* in use for FP32-bulk tone plans, -1 for other plans */
+    int32_t tile_intervals; /* output intervals per scheduling tile (a warp's, or a CTA's for the tensor path) */
 } spinsim_plan_info;
 
 /* Library version string. */

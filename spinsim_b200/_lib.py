@@ -26,7 +26,7 @@ c_vp = ctypes.c_void_p
 class PlanDesc(ctypes.Structure):
     _fields_ = [("spin_dim", c_i32), ("integration", c_i32), ("expo_half", c_i32), ("expo_one", c_i32),
                 ("rotating", c_i32), ("number_of_squares", c_i32), ("field_kind", c_i32), ("precision", c_i32),
-                ("threads_per_block", c_i32), ("max_registers", c_i32), ("lanes", c_i32), ("reserved", c_i32)]
+                ("threads_per_block", c_i32), ("max_registers", c_i32), ("lanes", c_i32), ("variant", c_i32)]
 
 
 class Table(ctypes.Structure):
@@ -46,7 +46,8 @@ class Instance(ctypes.Structure):
 
 class PlanInfo(ctypes.Structure):
     _fields_ = [("registers_per_thread", c_i32), ("threads_per_block", c_i32), ("blocks_per_sm", c_i32),
-                ("sm_count", c_i32), ("lanes", c_i32), ("linked", c_i32)]
+                ("sm_count", c_i32), ("lanes", c_i32), ("linked", c_i32), ("variant", c_i32),
+                ("tile_intervals", c_i32)]
 
 
 class SpinsimError(RuntimeError):

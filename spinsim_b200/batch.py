@@ -50,7 +50,8 @@ class Batch:
     per-instance built-in fields), ``integration_method``, ``exponentiation_half`` /
     ``exponentiation_one`` (defaults: analytic for spin half, Lie-Trotter for spin one, I:529-533),
     ``use_rotating_frame``, ``number_of_squares``, ``precision``, ``lanes``, ``threads_per_block``,
-    ``max_registers`` (the last three are picked by ``spinsim_b200.autotune.tune``), ``force_mixed``
+    ``max_registers``, ``variant`` (FP32-bulk tone fields: 0 the tensor-path kernel, 1 the warp
+    synthesis; these four are picked by ``spinsim_b200.autotune.tune``), ``force_mixed``
     (use the mixed-spin kernel even for a single-spin batch), ``memory`` (a callable taking a byte
     count and returning a 256-byte aligned uint8 CUDA tensor of at least that size; default
     ``torch.empty``).  All device buffers of the batch (outputs, workspace, fields, sweep
@@ -65,7 +66,7 @@ class Batch:
                  exponentiation_half=ExponentiationMethod.ANALYTIC, exponentiation_one=ExponentiationMethod.LIE_TROTTER,
                  use_rotating_frame=True, number_of_squares=24, precision=Precision.FP64, lanes=0,
                  threads_per_block=0, max_registers=0, plan_cache=None, force_mixed=False, memory=None,
-                 staging=None):
+                 staging=None, variant=0):
         import torch
         self.instances = list(instances)
         if not self.instances:
@@ -99,8 +100,9 @@ class Batch:
         desc.threads_per_block = int(threads_per_block)
         desc.lanes = int(lanes)
         desc.max_registers = int(max_registers)
+        desc.variant = int(variant)
         self.config = {"lanes": int(lanes), "threads_per_block": int(threads_per_block),
-                       "max_registers": int(max_registers)}
+                       "max_registers": int(max_registers), "variant": int(variant)}
         self.lib = lib = _lib.load()
         key = bytes(desc) + (ltoir or b"")
         if plan_cache is not None and key in plan_cache:

@@ -82,6 +82,8 @@ MINB = (2, 3, 4)
 # Tighter budgets (96 and 80 registers) for the FP32-bulk tabulated-field kernels, the serving path,
 # whose latency-bound table lookups gain from residency more than they lose to spills.
 MINB_TIGHT = (5, 6)
+# Register budgets of the tensor-path tone kernels (128-thread CTAs): 5 -> 102, 4 -> 128, 3 -> 168 registers.
+DMMA_MINB = (3, 4, 5)
 
 
 def gen_sources():
@@ -114,9 +116,25 @@ def gen_sources():
         reg_decl.append(f'extern "C" const unsigned char spinsim_blob_{name}_begin[], spinsim_blob_{name}_end[];')
         user_rows.append(f"    {{{v[0]}, {v[1]}, {v[2]}, {v[3]}, {v[4]}, spinsim_blob_{name}_begin, "
                          f"spinsim_blob_{name}_end}},")
+    # FP32-bulk tone kernels with the field samples on the FP64 tensor path (one per spin mix and
+    # register budget; the exponentiators do not enter them).
+    dmma_rows = []
+    for dims in (0, 2, 3):
+        for minb in DMMA_MINB:
+            name = f"dmma_d{dims}_b{minb}"
+            src = os.path.join(GEN, f"k_{name}.cu")
+            body = (f'#include "evolve_dmma.cuh"\n'
+                    f"namespace spinsim {{\ntemplate __global__ void evolve_dmma_kernel<{dims}, {minb}>(EvolveArgs);\n}}\n"
+                    f'extern "C" const void* spinsim_kget_{name}(void) {{\n'
+                    f"    return (const void*)&spinsim::evolve_dmma_kernel<{dims}, {minb}>;\n}}\n")
+            write_if_changed(src, body)
+            units.append(("sass", name, src))
+            reg_decl.append(f'extern "C" const void* spinsim_kget_{name}(void);')
+            dmma_rows.append(f"    {{{dims}, {minb}, spinsim_kget_{name}}},")
     reg = ("// generated by spinsim_b200/build.py\n" + "\n".join(reg_decl) +
            "\nstatic const BuiltinEntry kBuiltin[] = {\n" + "\n".join(builtin_rows) + "\n};\n"
-           "static const UserEntry kUser[] = {\n" + "\n".join(user_rows) + "\n};\n")
+           "static const UserEntry kUser[] = {\n" + "\n".join(user_rows) + "\n};\n"
+           "static const DmmaEntry kDmma[] = {\n" + "\n".join(dmma_rows) + "\n};\n")
     write_if_changed(os.path.join(GEN, "registry_gen.inc"), reg)
     return units
 

@@ -113,6 +113,12 @@ struct ToneShared {
     double2 uv[2][kSynthIntervals][2][kToneSlots];  // [buffer][interval][U or V][slot] G^i U, G^i V of the step
 };
 constexpr int kToneSharedBytes = kToneSlots * 32 * 2 * 8 + 2 * kToneSlots * kSynthIntervals * 4 * 8;
+// FP32-bulk tone kernel with the field samples on the FP64 tensor path (see evolve_dmma.cuh): a CTA
+// of kDmmaWarps warps takes a tile of kDmmaTile consecutive output intervals of one instance.
+constexpr int kDmmaWarps = 4;
+constexpr int kDmmaThreads = 32 * kDmmaWarps;
+constexpr int kDmmaRows = 8;                       // output intervals per warp (rows of m8n8k4)
+constexpr int kDmmaTile = kDmmaWarps * kDmmaRows;  // output intervals per CTA tile
 
 // ------------------------------------------------------------------ complex helpers (FP64)
 struct c64 {

@@ -155,8 +155,9 @@ SS_D void sample_field(const FieldDesc& f, double t, double* out, TableCursor* c
             double acc = f.bias[c];
             const double* tone = f.tones + 3 * f.tone_start[c];
             const int n = f.tone_count[c];
+            const double gain = f.gain[c];
             for (int k = 0; k < n; k++) {
-                const double w = __ldg(tone + 3 * k), a = __ldg(tone + 3 * k + 1), ph = __ldg(tone + 3 * k + 2);
+                const double w = __ldg(tone + 3 * k), a = gain * __ldg(tone + 3 * k + 1), ph = __ldg(tone + 3 * k + 2);
                 acc = fma(a, sin(fma(w, t, ph)), acc);
             }
             out[c] = acc;

@@ -93,14 +93,17 @@ def final_state_errors(a, b):
     return np.array([np.abs(x - y).max() if x.size else 0.0 for x, y in zip(a.final_states(), b.final_states())])
 
 
-def test_fp32_bulk_tones_error_vs_fp64(cuda):
-    """The batched FP32-bulk form against the plain FP64 form: final-state error <= 1e-6 (uneven
-    spin-half / spin-one tone batch, durations up to 2 ms)."""
+@pytest.mark.parametrize("variant", [0, 1])
+def test_fp32_bulk_tones_error_vs_fp64(cuda, variant):
+    """The batched FP32-bulk form (tensor-path kernel, variant 0, and warp synthesis, variant 1)
+    against the plain FP64 form: final-state error <= 1e-6 (uneven spin-half / spin-one tone batch,
+    durations up to 2 ms)."""
     import spinsim_b200 as ss
     import spinsim_b200.batch as B
     insts = make_instances(64, seed=11, max_duration=2e-3)
     plans = {}
-    bulk = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans)
+    bulk = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans, variant=variant)
+    assert bulk.plan_info()["variant"] == variant
     plain = B.Batch(insts, precision=ss.Precision.FP64, plan_cache=plans)
     bulk.run()
     plain.run()
@@ -251,6 +254,35 @@ def test_spin_mean_rejects_unequal_members(cuda):
     b.run()
     with pytest.raises(ValueError):
         b.spin_mean()
+
+
+def test_tensor_path_step_counts_and_tile_edges(cuda):
+    """The tensor-path tone kernel with every split of K fine steps over its four time segments
+    (K = 1 .. 9, 33, 100, 137: empty and uneven segments) and instance lengths that end inside a
+    CTA tile or a warp's rows, against the oracle and the warp-synthesis kernel."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    H, O1 = ss.SpinQuantumNumber.HALF, ss.SpinQuantumNumber.ONE
+    specs = []
+    for j, k in enumerate([1, 2, 3, 4, 5, 6, 7, 8, 9, 33, 100, 137]):
+        n = [1, 7, 8, 9, 31, 32, 33, 40, 65, 3, 12, 20][j]
+        specs.append((H if j % 3 else O1, 0.25e-6 * j, 0.25e-6 * j + n * 1e-6, 1e-6 / k, 1e-6))
+    insts = []
+    for j, (s, t0, t1, dti, dto) in enumerate(specs):
+        p = F.tone_parameters(np.random.default_rng(900 + j))
+        insts.append(B.Instance(s, t0, t1, dti, dto, s.plus_x, sweep_parameters=p, field=tone_field(p)))
+    plans = {}
+    tensor = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans, variant=0)
+    synth = B.Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans, variant=1)
+    tensor.run()
+    synth.run()
+    for k, (s, t0, t1, dti, dto) in enumerate(specs):
+        r, r1 = tensor.result(k), synth.result(k)
+        t, u, st, sp = O.evaluate(s.dimension, O.Field(8), insts[k].sweep_parameters, t0, t1, dti, dto, s.plus_x)
+        assert np.array_equal(r.time, t)
+        assert np.abs(r.time_evolution - u).max() < 1e-7, k
+        assert np.abs(r.state - st).max() < 1e-6, k
+        assert np.abs(r.state - r1.state).max() < 1e-6, k
 
 
 def test_ragged_batch_edge_instances(cuda):
