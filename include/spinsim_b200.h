@@ -252,6 +252,16 @@ int spinsim_batch_prepare_staged(const spinsim_plan* plan, const spinsim_instanc
                                  spinsim_batch** out);
 int spinsim_batch_launch(const spinsim_batch* batch, double* time_dev, double* u_dev, double* state_dev,
                          double* spin_dev, void* stream);
+
+/* The launch shape a prepared batch runs with (no counterpart in the reference): its tile queue,
+ * the output steps per tile, the lanes per output step, and the state scan's tiles. */
+typedef struct {
+    int64_t tiles;          /* time-evolution tiles in the queue */
+    int64_t scan_tiles;     /* state-scan tiles (with padding to whole warps) */
+    int32_t lanes;          /* lanes per output step */
+    int32_t tile_intervals; /* output steps per time-evolution tile */
+} spinsim_batch_info;
+int spinsim_batch_get_info(const spinsim_batch* batch, spinsim_batch_info* info);
 int spinsim_batch_destroy(spinsim_batch* batch);
 
 /* Diagnostics (no counterpart in the reference): one launch of an FMA-throughput loop that fills the

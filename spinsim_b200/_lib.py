@@ -50,6 +50,10 @@ class PlanInfo(ctypes.Structure):
                 ("tile_intervals", c_i32)]
 
 
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("tiles", c_i64), ("scan_tiles", c_i64), ("lanes", c_i32), ("tile_intervals", c_i32)]
+
+
 class SpinsimError(RuntimeError):
     """A failure reported by the CUDA library (message from spinsim_last_error)."""
 
@@ -96,6 +100,7 @@ _SIGNATURES = [
       ctypes.POINTER(c_vp)]),
     ("spinsim_batch_launch", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("spinsim_batch_destroy", ctypes.c_int, [c_vp]),
+    ("spinsim_batch_get_info", ctypes.c_int, [c_vp, ctypes.POINTER(BatchInfo)]),
     ("spinsim_fma_peak", ctypes.c_int, [c_i32, ctypes.POINTER(c_dbl), c_vp]),
     ("spinsim_state_static_max_steps", c_i64, []),
     ("spinsim_state_static", ctypes.c_int, [c_i32, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp]),

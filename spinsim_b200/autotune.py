@@ -1,8 +1,18 @@
-"""Autotuner for batched launches: picks lanes per output step, CTA size and register budget.
+"""Autotuner for batched launches: picks the time-evolution kernel's launch shape for a batch.
 
-For a given batch it times each candidate configuration once (after a warm-up launch) with CUDA
-events and keeps the fastest.  Results are cached per workload signature (spin mix, fine steps per
-output step, total output steps, precision, field kind) in a JSON file
+The candidates depend on the kernel the batch runs (``candidates_for``):
+
+* FP32-bulk tone fields: the kernel variant (0: field samples as FP64 tensor-core products over CTA
+  tiles of 32 output steps, 1: warp-synchronous phasor synthesis) and its register budget (which
+  sets the resident CTAs per SM), plus the CTA size for the warp-synchronous kernel; lanes per output
+  step do not apply (one lane per step, or a quad per step's time segments on the tensor path).
+* every other plan: lanes per output step, CTA size and register budget.
+
+Every candidate is a distinct launch.  For a given batch the tuner times each candidate after a
+warm-up launch with CUDA events and keeps the fastest; it returns the configuration and, in the
+timings, the launch that configuration produced (``plan_info``: registers, CTA size, CTAs per SM,
+lanes, kernel variant, tile size).  Results are cached per workload signature (spin mix, fine steps
+per output step, total output steps, precision, field kind) in a JSON file
 (``$SPINSIM_AUTOTUNE_CACHE``, default ``~/.cache/spinsim_b200/autotune.json``).
 """
 import hashlib
@@ -17,6 +27,20 @@ DEFAULT_CANDIDATES = [
     {"lanes": lanes, "threads_per_block": tpb, "max_registers": regs}
     for regs in (0, 168, 128) for lanes in (1, 2) for tpb in (64, 128)
 ]
+# FP32-bulk tone fields: tensor-path kernel at 102 (spills allowed), 128 and 168 registers; the warp
+# synthesis at 168 and 128 registers with 64- or 128-thread CTAs.
+BULK_TONE_CANDIDATES = (
+    [{"variant": 0, "max_registers": regs} for regs in (96, 128, 168)] +
+    [{"variant": 1, "max_registers": regs, "threads_per_block": tpb} for regs in (168, 128) for tpb in (64, 128)]
+)
+
+
+def candidates_for(instances, precision=None, get_field=None, **_):
+    """The distinct launch configurations worth timing for this batch."""
+    from . import Precision, ToneField
+    bulk = precision is not None and int(Precision(precision).value) == int(Precision.FP32_BULK.value)
+    tones = get_field is None and all(isinstance(i.field, ToneField) for i in instances)
+    return BULK_TONE_CANDIDATES if (bulk and tones) else DEFAULT_CANDIDATES
 
 
 def cache_path():
@@ -65,14 +89,22 @@ def tune(instances, candidates=None, use_cache=True, repeats=2, **batch_kwargs):
             hit = _load().get(sig)
         if hit:
             return hit["best"], hit["timings"]
-    candidates = candidates or DEFAULT_CANDIDATES
+    candidates = candidates or candidates_for(instances, **batch_kwargs)
     timings = {}
     best, best_t = None, float("inf")
+    seen = set()
     for cfg in candidates:
         try:
             b = Batch(instances, **batch_kwargs, **cfg)
         except (ValueError, NotImplementedError):
             continue
+        info = b.launch_info()
+        launch = (info["registers_per_thread"], info["threads_per_block"], info["blocks_per_sm"], info["lanes"],
+                  info["variant"], info["tile_intervals"])
+        if launch in seen:  # the same kernel and launch shape as a candidate already timed
+            del b
+            continue
+        seen.add(launch)
         b.run(with_state=False)
         torch.cuda.synchronize()
         ts = []
@@ -85,7 +117,7 @@ def tune(instances, candidates=None, use_cache=True, repeats=2, **batch_kwargs):
             torch.cuda.synchronize()
             ts.append(s.elapsed_time(e) / 1e3)
         t = min(ts)
-        timings[json.dumps(cfg, sort_keys=True)] = t
+        timings[json.dumps(cfg, sort_keys=True)] = {"seconds": t, "launch": info}
         if t < best_t:
             best, best_t = cfg, t
         del b

@@ -260,6 +260,17 @@ class Batch:
         _lib.check(self.lib.spinsim_plan_get_info(self._plan, ctypes.byref(info)))
         return {k: getattr(info, k) for k, _ in _lib.PlanInfo._fields_}
 
+    def launch_info(self):
+        """The launch this batch makes: the plan's kernel (plan_info) and the batch's tile queue,
+        tile size, lanes per output step and state-scan tiles."""
+        info = _lib.BatchInfo()
+        _lib.check(self.lib.spinsim_batch_get_info(self._handle, ctypes.byref(info)))
+        return {**self.plan_info(), **{k: getattr(info, k) for k, _ in _lib.BatchInfo._fields_}}
+
+    @property
+    def lanes(self):
+        return self.launch_info()["lanes"]
+
     def _restrict_to_pieces(self):
         """Apply the instances' ``intervals`` (first, count) to the descriptors and re-pack the
         output offsets; returns the new totals (output steps, U doubles, state doubles)."""

@@ -90,13 +90,14 @@ struct MethodConfig {
     double precision;       // 4 ** hypercubes  (I:1550)
 };
 
+// Launch arguments of the time-evolution kernels.
 struct EvolveArgs {
     MethodConfig m;
     const Instance* instances;
     const FieldDesc* fields;
-    const Tile* tiles;       // null: single instance, implicit tiles of 32 / lanes intervals
+    const Tile* tiles;       // null: single instance, implicit tiles of 32 / lanes intervals (a CTA's 32 on the tensor path)
     int64_t n_tiles;
-    int32_t* tile_counter;   // null: one tile per warp of the grid, no queue
+    int32_t* tile_counter;   // null: one tile per warp (per CTA on the tensor path) of the grid, no queue
     double* time;            // [sum N]
     double* u;               // complex [sum N * d * d]; instance i starts at u_offset doubles
 };
@@ -206,5 +207,34 @@ SS_HD Mat<D> multiply_m1(const Mat<D>& l, const Mat<D>& r) {
         }
     return o;
 }
+
+#ifdef __CUDACC__
+// Warp shuffles of a whole operator (every lane of the warp must take part).
+template <int D>
+__device__ __forceinline__ Mat<D> shfl_down_mat(const Mat<D>& m, int delta) {
+    Mat<D> o;
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            o.a[i][j].re = __shfl_down_sync(0xffffffffu, m.a[i][j].re, delta);
+            o.a[i][j].im = __shfl_down_sync(0xffffffffu, m.a[i][j].im, delta);
+        }
+    return o;
+}
+
+template <int D>
+__device__ __forceinline__ Mat<D> shfl_up_mat(const Mat<D>& m, int delta) {
+    Mat<D> o;
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            o.a[i][j].re = __shfl_up_sync(0xffffffffu, m.a[i][j].re, delta);
+            o.a[i][j].im = __shfl_up_sync(0xffffffffu, m.a[i][j].im, delta);
+        }
+    return o;
+}
+#endif
 
 }  // namespace spinsim

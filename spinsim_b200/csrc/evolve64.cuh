@@ -59,19 +59,6 @@ SS_D void transform_frame64(double* s, double rw, c64 w) {
     }
 }
 
-template <int D>
-SS_D Mat<D> shfl_down_mat(const Mat<D>& m, int delta) {
-    Mat<D> o;
-#pragma unroll
-    for (int i = 0; i < D; i++)
-#pragma unroll
-        for (int j = 0; j < D; j++) {
-            o.a[i][j].re = __shfl_down_sync(0xffffffffu, m.a[i][j].re, delta);
-            o.a[i][j].im = __shfl_down_sync(0xffffffffu, m.a[i][j].im, delta);
-        }
-    return o;
-}
-
 // Evolve one output interval.  Every lane of the warp must call this (shuffles use the full mask);
 // lanes with `active == false` do no steps and write nothing.
 template <int D, int INTEG, int EXPO, int FIELD>

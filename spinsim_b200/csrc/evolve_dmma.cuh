@@ -324,33 +324,34 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
         const Su2d later = shfl_down_su2(acc, sft);
         if ((q & (2 * sft - 1)) == 0) acc = su2d_mul(later, acc);
     }
-    if (!active || q != 0) return;
-    const c64 alpha = c64{1.0 + acc.am1.re, acc.am1.im};
-    Mat<D> u;
-    if constexpr (D == 3) {
-        u = su2_to_spin_one(alpha, acc.beta);
-    } else {
-        u.a[0][0] = alpha;
-        u.a[1][0] = acc.beta;
-        u.a[0][1] = c64{-acc.beta.re, acc.beta.im};
-        u.a[1][1] = conj(alpha);
-    }
-    if (m.rotating) {  // leave the rotating frame, I:839-852
-        c64 wo;
-        sincos(rw * dt_out, &wo.im, &wo.re);
-        const c64 woc = conj(wo);
-#pragma unroll
-        for (int k = 0; k < D; k++) {
-            u.a[0][k] = u.a[0][k] * woc;
-            u.a[D - 1][k] = u.a[D - 1][k] * wo;
+    if (active && q == 0) {
+        Mat<D> u;  // lab-frame operator of the interval
+        const c64 alpha = c64{1.0 + acc.am1.re, acc.am1.im};
+        if constexpr (D == 3) {
+            u = su2_to_spin_one(alpha, acc.beta);
+        } else {
+            u.a[0][0] = alpha;
+            u.a[1][0] = acc.beta;
+            u.a[0][1] = c64{-acc.beta.re, acc.beta.im};
+            u.a[1][1] = conj(alpha);
         }
+        if (m.rotating) {  // leave the rotating frame, I:839-852
+            c64 wo;
+            sincos(rw * dt_out, &wo.im, &wo.re);
+            const c64 woc = conj(wo);
+#pragma unroll
+            for (int k = 0; k < D; k++) {
+                u.a[0][k] = u.a[0][k] * woc;
+                u.a[D - 1][k] = u.a[D - 1][k] * wo;
+            }
+        }
+        time_out[idx] = t_c;
+        double2* dst = reinterpret_cast<double2*>(u_out) + idx * (D * D);
+#pragma unroll
+        for (int r = 0; r < D; r++)
+#pragma unroll
+            for (int k = 0; k < D; k++) dst[r * D + k] = make_double2(u.a[r][k].re, u.a[r][k].im);
     }
-    time_out[idx] = t_c;
-    double2* dst = reinterpret_cast<double2*>(u_out) + idx * (D * D);
-#pragma unroll
-    for (int r = 0; r < D; r++)
-#pragma unroll
-        for (int k = 0; k < D; k++) dst[r * D + k] = make_double2(u.a[r][k].re, u.a[r][k].im);
 }
 
 // Persistent launch: CTAs pull tiles of kDmmaTile intervals from the queue (or, without a queue, CTA

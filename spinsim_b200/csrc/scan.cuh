@@ -3,23 +3,29 @@
 // The reference propagates the state serially on the host (get_state, spinsim/__init__.py:1089-1111):
 //     state[0] = psi0,   state[i] = U[i-1] state[i-1]
 // i.e. state[i] = (U[i-1] ... U[0]) psi0 and the last operator is never applied.  Here that is a
-// parallel prefix scan of the d x d operators in FP64, in three launches with no inter-block waits:
-//   A  scan_reduce_kernel: each CTA takes a scan tile of kScanThreads * kScanChunk consecutive
-//      intervals of one instance; thread t multiplies its kScanChunk operators, the CTA scans the
-//      thread products in shared memory and stores each thread's exclusive in-tile prefix and the
-//      tile product.
-//   B  scan_tiles_kernel: one thread per instance walks its tiles in order and stores the
-//      exclusive prefix of every tile (and, when asked, the instance's whole product).
-//   C  scan_apply_kernel: thread t forms prefix = (in-tile prefix) (tile prefix), applies it to psi0
-//      and walks its chunk writing state and spin (get_spin, I:899-959), fused.
+// parallel prefix scan of the d x d operators in FP64 over scan tiles of kScanTile consecutive
+// output steps of one instance (one warp each), with no waits between blocks:
+// A tile is taken by an 8-lane group (four tiles per warp); lane j of the group holds the product of
+// the tile's operators 4 j .. 4 j + 3, so a tile costs three shuffle rounds instead of five.
+//   A  scan_products_kernel: each group multiplies its tile's operators into the tile product.
+//   B  scan_prefix_kernel: a warp per instance scans the instance's tile products 32 at a time and
+//      stores every tile's exclusive prefix (and, when asked, the instance's whole product).
+//   C  scan_apply_kernel: each group scans its lanes' products (lane j: U[4j+3] ... U[0] of the
+//      tile), applies the exclusive part times the tile's prefix to psi0 and steps through its
+//      four output steps writing state and spin (get_spin, I:899-959), fused.
+// Spin half and spin one instances share the launches; the tile list holds the spin-half tiles, then
+// the spin-one tiles, each run padded to whole warps (count 0), so a warp's tiles share a dimension.
 #pragma once
 #include "common.cuh"
 
 namespace spinsim {
 
-constexpr int kScanThreads = 256;
-constexpr int kScanChunk = 8;
-constexpr int kScanTile = kScanThreads * kScanChunk;
+constexpr int kScanTile = 32;        // output steps per scan tile
+constexpr int kScanPerLane = 4;      // consecutive operators multiplied by one lane
+constexpr int kScanGroup = kScanTile / kScanPerLane;  // lanes per tile (8)
+constexpr int kScanTilesPerWarp = 32 / kScanGroup;    // 4
+constexpr int kScanMat = 18;         // doubles per stored tile operator (3 x 3 complex; spin half uses 8)
+constexpr int kScanBlock = 128;      // threads per CTA of the scan kernels
 
 template <int D>
 SS_D Mat<D> load_mat(const double* p) {
@@ -62,133 +68,206 @@ SS_D void spin_of(const c64* s, double* out) {
     }
 }
 
-// Scan tiles: tile -> (instance, first interval, count); instance-local.
+#ifdef __CUDACC__
+// Inclusive scan: lane i receives M[i] ... M[0].
+template <int D>
+SS_D Mat<D> warp_scan(Mat<D> m, int lane) {
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        const Mat<D> earlier = shfl_up_mat(m, s);
+        if (lane >= s) m = matmul(m, earlier);
+    }
+    return m;
+}
+#endif
+
+// Scan tiles: tile -> (instance, first output step, count).  Without a tile list (tiles == null) the
+// launch covers one instance, instances[0], with implicit tiles of kScanTile steps.
 struct ScanArgs {
     const Instance* instances;
-    const Tile* tiles;       // scan tiles (kScanTile intervals max), grouped by instance, in order
+    const Tile* tiles;          // scan tiles, grouped by instance in order; null: implicit tiles
     int64_t n_tiles;
-    const int32_t* tile_begin;  // per instance: first scan tile index (instances with this dim only)
+    const int32_t* tile_begin;  // per instance: first scan tile (implicit for a single instance)
     const int32_t* tile_end;
     int32_t n_instances;
-    const double* u;          // operators, FP64 complex
-    double* thread_prefix;    // [n_tiles][kScanThreads][D][D] complex: exclusive in-tile prefixes
-    double* tile_product;     // [n_tiles][D][D] complex
-    double* tile_prefix;      // [n_tiles][D][D] complex
-    double* state;            // complex [sum N * d]
-    double* spin;             // [sum N * 3], may be null
-    double* total;            // per instance (of this dim): U[N-1] ... U[0], complex [D][D]; may be null
+    const double* u;            // operators, FP64 complex
+    double* tile_product;       // [n_tiles][kScanMat]
+    double* tile_prefix;        // [n_tiles][kScanMat]
+    double* state;              // complex [sum N * d]
+    double* spin;               // [sum N * 3], may be null
+    double* total;              // per instance: U[N-1] ... U[0], complex [d][d]; may be null
+    int64_t single_n_out;       // output steps of the single instance (implicit tiles)
 };
 
+SS_D const Instance& scan_instance(const ScanArgs& a, int32_t i) { return a.instances[i]; }
+
+// Tile k, or an empty tile (count 0) past the end of the list.
+SS_D Tile scan_tile(const ScanArgs& a, int64_t k) {
+    Tile t;
+    t.instance = 0;
+    t.first = 0;
+    t.count = 0;
+    if (k >= a.n_tiles) return t;
+    if (a.tiles != nullptr) return a.tiles[k];
+    t.first = k * kScanTile;
+    const int64_t rest = a.single_n_out - t.first;
+    t.count = (int32_t)(rest < kScanTile ? rest : kScanTile);
+    return t;
+}
+
+// Writes a single call's instance (and field) descriptors into its workspace from the launch's own
+// arguments: no host-to-device copy, so the call stays stream-ordered and capturable.
+struct DescriptorArgs {
+    Instance inst;
+    FieldDesc field;
+    Instance* inst_dst;
+    FieldDesc* field_dst;  // may be null
+};
+
+#ifdef __CUDACC__
+// Lane j of the tile's group: U[4j + 3] ... U[4j] of the tile (identity past its end).
 template <int D>
-__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(ScanArgs a) {
-    constexpr int MD = 2 * D * D;  // doubles per matrix
-    __shared__ double sh[kScanThreads * MD];
-    const int64_t tile_id = blockIdx.x;
-    if (tile_id >= a.n_tiles) return;
-    const Tile tile = a.tiles[tile_id];
-    const Instance& inst = a.instances[tile.instance];
-    const double* u = a.u + inst.u_offset + (tile.first) * MD;
-    const int t = threadIdx.x;
-    const int lo = t * kScanChunk;
-    int hi = lo + kScanChunk;
-    if (hi > tile.count) hi = tile.count;
+SS_D Mat<D> lane_operators(const ScanArgs& a, const Instance& inst, const Tile& tile, int j) {
+    constexpr int MD = 2 * D * D;
+    const double* u = a.u + inst.u_offset + (tile.first + kScanPerLane * j) * MD;
+    const int n = min(kScanPerLane, tile.count - kScanPerLane * j);
     Mat<D> p;
-    set_identity(p);
-    for (int i = lo; i < hi; i++) p = matmul(load_mat<D>(u + (int64_t)i * MD), p);
-    // Hillis-Steele inclusive scan over threads: incl[t] = p[t] p[t-1] ... p[0]
-    store_mat<D>(sh + t * MD, p);
-    __syncthreads();
-    for (int off = 1; off < kScanThreads; off <<= 1) {
-        Mat<D> earlier;
-        const bool take = t >= off;
-        if (take) {
+    if (n > 0) p = load_mat<D>(u);
+    else set_identity(p);
 #pragma unroll
-            for (int i = 0; i < D; i++)
-#pragma unroll
-                for (int j = 0; j < D; j++)
-                    earlier.a[i][j] = c64{sh[(t - off) * MD + 2 * (i * D + j)], sh[(t - off) * MD + 2 * (i * D + j) + 1]};
-        }
-        __syncthreads();
-        if (take) {
-            p = matmul(p, earlier);
-            store_mat<D>(sh + t * MD, p);
-        }
-        __syncthreads();
-    }
-    // exclusive prefix for thread t = inclusive of t - 1
-    Mat<D> ex;
-    if (t == 0) {
-        set_identity(ex);
-    } else {
-#pragma unroll
-        for (int i = 0; i < D; i++)
-#pragma unroll
-            for (int j = 0; j < D; j++)
-                ex.a[i][j] = c64{sh[(t - 1) * MD + 2 * (i * D + j)], sh[(t - 1) * MD + 2 * (i * D + j) + 1]};
-    }
-    store_mat<D>(a.thread_prefix + (tile_id * kScanThreads + t) * MD, ex);
-    if (t == kScanThreads - 1) store_mat<D>(a.tile_product + tile_id * MD, p);
+    for (int i = 1; i < kScanPerLane; i++)
+        if (i < n) p = matmul(load_mat<D>(u + i * MD), p);
+    return p;
 }
 
 template <int D>
-__global__ void scan_tiles_kernel(ScanArgs a) {
-    constexpr int MD = 2 * D * D;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n_instances) return;
+SS_D void products_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) {
+    Mat<D> m;
+    if (tile.count > 0) m = lane_operators<D>(a, scan_instance(a, tile.instance), tile, j);
+    else set_identity(m);
+#pragma unroll
+    for (int s = 1; s < kScanGroup; s <<= 1) {  // tree over the group's lanes, later ones from the left
+        const Mat<D> later = shfl_down_mat(m, s);
+        if ((j & (2 * s - 1)) == 0) m = matmul(later, m);
+    }
+    if (j == 0 && tile.count > 0) store_mat<D>(a.tile_product + k * kScanMat, m);
+}
+
+// The dimension of a warp's tiles (all its tiles share it; the first is never a padding tile).
+SS_D int warp_dim(const ScanArgs& a, int64_t first_tile) {
+    const Tile t = scan_tile(a, first_tile);
+    return t.count > 0 ? scan_instance(a, t.instance).dim : 2;
+}
+
+#ifdef SPINSIM_SCAN_KERNELS  // the launches themselves are defined once, in the C ABI's unit
+__global__ void put_descriptors_kernel(DescriptorArgs a) {
+    if (threadIdx.x == 0) {
+        *a.inst_dst = a.inst;
+        if (a.field_dst != nullptr) *a.field_dst = a.field;
+    }
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_products_kernel(ScanArgs a) {
+    const int64_t w = ((int64_t)blockIdx.x * kScanBlock + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t k = w * kScanTilesPerWarp + lane / kScanGroup;
+    if (w * kScanTilesPerWarp >= a.n_tiles) return;
+    const Tile tile = scan_tile(a, k);
+    if (warp_dim(a, w * kScanTilesPerWarp) == 2) products_group<2>(a, tile, k, lane % kScanGroup);
+    else products_group<3>(a, tile, k, lane % kScanGroup);
+}
+
+#endif
+
+template <int D>
+SS_D void prefix_warp(const ScanArgs& a, int32_t i, int lane) {
+    const int32_t b = a.tile_begin != nullptr ? a.tile_begin[i] : 0;
+    const int32_t e = a.tile_end != nullptr ? a.tile_end[i] : (int32_t)a.n_tiles;
     Mat<D> run;
     set_identity(run);
-    for (int k = a.tile_begin[i]; k < a.tile_end[i]; k++) {
-        store_mat<D>(a.tile_prefix + (int64_t)k * MD, run);
-        run = matmul(load_mat<D>(a.tile_product + (int64_t)k * MD), run);
+    for (int32_t c0 = b; c0 < e; c0 += 32) {
+        const int32_t k = c0 + lane;
+        Mat<D> p;
+        if (k < e) p = load_mat<D>(a.tile_product + (int64_t)k * kScanMat);
+        else set_identity(p);
+        const Mat<D> incl = warp_scan<D>(p, lane);
+        Mat<D> excl = shfl_up_mat(incl, 1);
+        if (lane == 0) set_identity(excl);
+        if (k < e) store_mat<D>(a.tile_prefix + (int64_t)k * kScanMat, matmul(excl, run));
+        run = matmul(shfl_down_mat(incl, 31 - lane), run);  // lane 31's inclusive product (a full chunk)
     }
-    if (a.total) store_mat<D>(a.total + (int64_t)i * MD, run);
+    if (a.total != nullptr && lane == 0) store_mat<D>(a.total + (int64_t)i * 2 * D * D, run);
 }
 
+#ifdef SPINSIM_SCAN_KERNELS
+__global__ void __launch_bounds__(kScanBlock) scan_prefix_kernel(ScanArgs a) {
+    const int32_t i = (int32_t)(((int64_t)blockIdx.x * kScanBlock + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= a.n_instances) return;
+    if (scan_instance(a, i).dim == 2) prefix_warp<2>(a, i, lane);
+    else prefix_warp<3>(a, i, lane);
+}
+
+#endif
+
 template <int D>
-__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(ScanArgs a) {
+SS_D void apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) {
     constexpr int MD = 2 * D * D;
-    const int64_t tile_id = blockIdx.x;
-    if (tile_id >= a.n_tiles) return;
-    const Tile tile = a.tiles[tile_id];
-    const Instance& inst = a.instances[tile.instance];
-    const int t = threadIdx.x;
-    const int lo = t * kScanChunk;
-    if (lo >= tile.count) return;
-    int hi = lo + kScanChunk;
-    if (hi > tile.count) hi = tile.count;
-    const Mat<D> pre = matmul(load_mat<D>(a.thread_prefix + (tile_id * kScanThreads + t) * MD),
-                              load_mat<D>(a.tile_prefix + tile_id * MD));
-    c64 psi[D], v[D];
+    const Instance& inst = scan_instance(a, tile.instance);
+    Mat<D> m;
+    if (tile.count > 0) m = lane_operators<D>(a, inst, tile, j);
+    else set_identity(m);
 #pragma unroll
-    for (int k = 0; k < D; k++) v[k] = c64{inst.psi0[2 * k], inst.psi0[2 * k + 1]};
+    for (int s = 1; s < kScanGroup; s <<= 1) {  // inclusive scan over the group's lanes
+        const Mat<D> earlier = shfl_up_mat(m, s);
+        if (j >= s) m = matmul(m, earlier);
+    }
+    Mat<D> excl = shfl_up_mat(m, 1);
+    if (j == 0) set_identity(excl);
+    const int first = kScanPerLane * j;
+    if (tile.count <= first) return;
+    // psi = (exclusive prefix) (tile prefix) psi0 at output step `first`, then the next three steps
+    const Mat<D> pre = load_mat<D>(a.tile_prefix + k * kScanMat);
+    c64 v[D], psi[D];
 #pragma unroll
     for (int r = 0; r < D; r++) {
-        c64 acc = pre.a[r][0] * v[0];
+        c64 acc = c64{0.0, 0.0};
 #pragma unroll
-        for (int k = 1; k < D; k++) acc = cfma(pre.a[r][k], v[k], acc);
+        for (int c = 0; c < D; c++) acc = cfma(pre.a[r][c], c64{inst.psi0[2 * c], inst.psi0[2 * c + 1]}, acc);
+        v[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < D; r++) {
+        c64 acc = excl.a[r][0] * v[0];
+#pragma unroll
+        for (int c = 1; c < D; c++) acc = cfma(excl.a[r][c], v[c], acc);
         psi[r] = acc;
     }
-    const double* u = a.u + inst.u_offset + tile.first * MD;
-    double2* st = reinterpret_cast<double2*>(a.state + inst.state_offset) + tile.first * D;
-    double* sp = a.spin ? a.spin + (inst.out_offset + tile.first) * 3 : nullptr;
-    for (int i = lo; i < hi; i++) {
+    const int64_t i0 = tile.first + first;
+    const double* u = a.u + inst.u_offset + i0 * MD;
+    double2* st = reinterpret_cast<double2*>(a.state + inst.state_offset) + i0 * D;
+    double* sp = a.spin != nullptr ? a.spin + (inst.out_offset + i0) * 3 : nullptr;
+    const int n = min(kScanPerLane, tile.count - first);
 #pragma unroll
-        for (int k = 0; k < D; k++) st[(int64_t)i * D + k] = make_double2(psi[k].re, psi[k].im);
-        if (sp) {
+    for (int i = 0; i < kScanPerLane; i++) {
+        if (i >= n) break;
+#pragma unroll
+        for (int r = 0; r < D; r++) st[i * D + r] = make_double2(psi[r].re, psi[r].im);
+        if (sp != nullptr) {
             double s3[3];
             spin_of<D>(psi, s3);
-            sp[(int64_t)i * 3 + 0] = s3[0];
-            sp[(int64_t)i * 3 + 1] = s3[1];
-            sp[(int64_t)i * 3 + 2] = s3[2];
+            sp[3 * i + 0] = s3[0];
+            sp[3 * i + 1] = s3[1];
+            sp[3 * i + 2] = s3[2];
         }
-        if (i + 1 < hi) {
-            const Mat<D> m = load_mat<D>(u + (int64_t)i * MD);
+        if (i + 1 < n) {
+            const Mat<D> op = load_mat<D>(u + i * MD);
             c64 nx[D];
 #pragma unroll
             for (int r = 0; r < D; r++) {
-                c64 acc = m.a[r][0] * psi[0];
+                c64 acc = op.a[r][0] * psi[0];
 #pragma unroll
-                for (int k = 1; k < D; k++) acc = cfma(m.a[r][k], psi[k], acc);
+                for (int c = 1; c < D; c++) acc = cfma(op.a[r][c], psi[c], acc);
                 nx[r] = acc;
             }
 #pragma unroll
@@ -197,6 +276,20 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(ScanArgs a) {
     }
 }
 
+#ifdef SPINSIM_SCAN_KERNELS
+__global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(ScanArgs a) {
+    const int64_t w = ((int64_t)blockIdx.x * kScanBlock + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t k = w * kScanTilesPerWarp + lane / kScanGroup;
+    if (w * kScanTilesPerWarp >= a.n_tiles) return;
+    const Tile tile = scan_tile(a, k);
+    if (warp_dim(a, w * kScanTilesPerWarp) == 2) apply_group<2>(a, tile, k, lane % kScanGroup);
+    else apply_group<3>(a, tile, k, lane % kScanGroup);
+}
+#endif  // SPINSIM_SCAN_KERNELS
+#endif
+
+#ifdef SPINSIM_SCAN_KERNELS
 // Standalone get_spin (I:899-959) for a state series: spin[i] from state[i].
 template <int D>
 __global__ void spin_kernel(const double* state, int64_t n, double* spin) {
@@ -252,5 +345,7 @@ __global__ void __launch_bounds__(kMeanThreads) spin_mean_final_kernel(const dou
     for (int c = 0; c < chunks; c++) s += partial[(int64_t)c * n_out * 3 + k];
     mean[k] = s / (double)members;
 }
+
+#endif  // SPINSIM_SCAN_KERNELS
 
 }  // namespace spinsim

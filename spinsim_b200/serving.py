@@ -82,9 +82,10 @@ class Request:
 
         Outputs (time 8, U 16 d^2, state 16 d, spin 24 bytes per output step); the launch workspace
         (a 120-byte instance and 224-byte field descriptor, time-evolution tiles of 16 bytes per 32
-        steps at most, and per scan tile of 2,048 steps a 16-byte tile, 256 thread prefixes and two
-        tile products of 16 d^2 bytes each); the field (tables or tones, 32-byte aligned chunks, and
-        eight 32-byte table descriptors); 256-byte alignment of every piece."""
+        steps at most, and per scan tile of 32 steps a 16-byte tile and two 144-byte operators: the
+        tile's product and prefix, 9.5 bytes per step, counted as 3 d^2); the field (tables or tones,
+        32-byte aligned chunks, and eight 32-byte table descriptors); 256-byte alignment of every
+        piece."""
         d = self.spin.dimension
         n = max(0, int((float(self.time_end) - float(self.time_start)) / float(self.time_step_output)))
         fld = 256

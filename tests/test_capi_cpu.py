@@ -68,10 +68,13 @@ def test_workspace_sizes():
     assert lib.spinsim_state_workspace_size(2, 0) > 0
     a = lib.spinsim_state_workspace_size(2, 200_000)
     b = lib.spinsim_state_workspace_size(3, 200_000)
-    assert 0 < a < b
+    assert 0 < a <= b
     assert lib.spinsim_state_workspace_size(4, 10) == 0
-    # per-thread in-tile prefixes: one d x d matrix per 8 intervals, plus per-tile matrices
-    assert a >= 200_000 // 8 * 64
+    # two stored operators (tile product and prefix, 3 x 3 complex slots) per scan tile of 32 steps
+    assert a >= (200_000 // 32) * 2 * 144
+    assert lib.spinsim_state_workspace_size(2, 33) > lib.spinsim_state_workspace_size(2, 32)
+    # the fixed scratch of spinsim_state_static holds the scan of its largest input
+    assert lib.spinsim_state_workspace_size(3, lib.spinsim_state_static_max_steps()) <= 5 << 20
 
 
 def test_state_entry_points_check_arguments_without_a_gpu():

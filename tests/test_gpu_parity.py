@@ -165,7 +165,7 @@ def test_gaussian_ensemble_members_full_length(cuda):
 
 
 @pytest.mark.parametrize("dim", [2, 3])
-@pytest.mark.parametrize("n", [1, 2, 2047, 2048, 2049, 300_001])
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 1023, 1024, 1025, 32_769, 300_001])
 def test_state_scan_matches_serial_propagation(cuda, dim, n):
     """get_state as a prefix scan against the reference's serial loop (I:1089-1111) on random
     unitaries, across scan-tile boundaries."""
