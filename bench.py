@@ -76,12 +76,13 @@ def instances(ss, specs):
 # is 2 flops; sin, cos, sqrt and division count 1 each).  Plain FP64, spin half: field 192 + 48 sin,
 # windings 8 + 4 sincos, frame 24, generators 24, two analytic exponentials 40 + 8, two 2x2 complex
 # products 128, time 1.  Spin one (Lie-Trotter, 24 squarings): field 192 + 48, windings 8 + 4,
-# frame 14, generators 32, two exponentials 10,920 + 14, two 3x3 products 432, time 1.  FP32-bulk:
-# tone synthesis 192 (two FMAs per tone and Gauss point) + producer share 9 + sums 6, frame 32,
-# generators 18 (24 for spin one), SU(2) product 32, time 1 in FP64; two SU(2) exponentials and their
-# product 90 in FP32.
+# frame 14, generators 32, two exponentials 10,920 + 14, two 3x3 products 432, time 1.  FP32-bulk
+# (tensor-path tone kernel, Magnus step): field samples 192 as FP64 tensor-core products (two Gauss
+# points x three channels x 16 multiply-adds) + the phasor table's recurrences 9, frame 26, sum and
+# difference of the samples 6, the SU(2) product into the interval's FP64 operator 33; in FP32 the
+# commutator 15 and one SU(2) exponential 27.  Spin one runs as SU(2) (no quadratic shift here).
 FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
-FLOPS_BULK = {2: {"fp64": 290, "fp32": 90}, 3: {"fp64": 296, "fp32": 90}}
+FLOPS_BULK = {2: {"fp64": 266, "fp32": 42}, 3: {"fp64": 266, "fp32": 42}}
 # DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload
 # (max_registers 168, state scan not run), from one capture of
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve -c 1`.
@@ -301,7 +302,7 @@ def bench_ours(args, world, rank):
         del res
     e2e_total = barrier_max(sum(e2e_times), world)
 
-    info = bulk.plan_info()
+    info = bulk.launch_info()
     peaks = peaks_from_file()
     fp64_flops, fp32_flops = algorithmic_flops(specs, "bulk")
     evolve_s = float(np.mean(t_evolve))
@@ -327,10 +328,11 @@ def bench_ours(args, world, rank):
                                "Magnus CF4, rotating frame, one persistent launch (CUDA graph)",
                    "instances_per_gpu": len(specs), "integration_steps_per_gpu": total_steps,
                    "l2": "256 MB buffer written between timed steps",
-                   "autotuned": {"fp32_bulk": cfg_bulk, "fp64": cfg_plain},
+                   "autotuned": {"fp32_bulk": {"chosen": cfg_bulk, "launched": bulk.launch_info()},
+                                 "fp64": {"chosen": cfg_plain, "launched": plain.launch_info()}},
                    "threads_per_block": info["threads_per_block"], "registers": info["registers_per_thread"],
-                   "tuning_ms": {"fp32_bulk": {k: 1e3 * v for k, v in tune_bulk.items()},
-                                 "fp64": {k: 1e3 * v for k, v in tune_plain.items()}}},
+                   "tuning_ms": {"fp32_bulk": {k: 1e3 * v["seconds"] for k, v in tune_bulk.items()},
+                                 "fp64": {k: 1e3 * v["seconds"] for k, v in tune_plain.items()}}},
         "latency_ms": {"p50": 1e3 * float(np.percentile(t_bulk, 50)), "p99": 1e3 * float(np.percentile(t_bulk, 99))},
         "plain_fp64": {"value": world * total_steps * args.steps / t_plain_total, "unit": "steps/s",
                        "ms_per_step": 1e3 * t_plain_total / args.steps,
@@ -346,7 +348,8 @@ def bench_ours(args, world, rank):
                      "peak_source": fp64_peak["source"],
                      "fp32_achieved": fp32_flops / evolve_s / 1e12,
                      "kernel_ms": 1e3 * evolve_s},
-        "gpu_launches": 7 * args.steps,
+        # per timed step: the time-evolution kernel and the scan's products, prefix and apply kernels
+        "gpu_launches": 4 * args.steps,
         "clocks": clocks.summary(),
         "e2e": {"value": world * total_steps * len(e2e_times) / e2e_total, "unit": "steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -394,36 +397,37 @@ def host_threads():
 
 
 def bench_reference(args, world, rank):
+    """The reference's CPU algorithm (the oracle: the reference's get_time_evolution and get_state,
+    restated in C with OpenMP over output steps as the reference's CPU device parallelises them) on
+    the whole benchmark batch every step: every instance's time evolution, then its state
+    propagation (I:1081-1082), on all host threads."""
     from oracle import oracle as O
     specs = workload(seed_base=0)
     O.lib()
     threads = host_threads()
-    times, steps_list = [], []
-    _, _, frac = cpu_sample(specs, seconds_target=min(8.0, 120.0 / max(1, args.steps + args.warmup)),
-                            n_threads=threads)
     field = O.Field(8)
+    total = sum(int(dur / 1e-6) * 100 for _, dur, _ in specs)
+    times = []
     for it in range(args.warmup + args.steps):
-        steps = 0
         t0 = time.perf_counter()
         for dim, dur, p in specs:
             n = int(dur / 1e-6)
-            cnt = max(1, int(n * frac)) if n else 0
-            if cnt:
-                O.time_evolution(dim, field, p, 0.0, 10e-9, 1e-6, n, first=0, count=cnt, n_threads=threads)
-                steps += cnt * 100
+            if n:
+                _, u = O.time_evolution(dim, field, p, 0.0, 10e-9, 1e-6, n, n_threads=threads)
+                O.state(u, np.array([1, 0], complex) if dim == 2 else np.array([0.5, 0.5 ** 0.5, 0.5], complex))
         el = time.perf_counter() - t0
         if it >= args.warmup:
             times.append(el)
-            steps_list.append(steps)
-    value = sum(steps_list) / sum(times)
-    sample = (f"first {frac:.4f} of the output intervals of each of the {len(specs)} instances "
-              f"({steps_list[0]} integration steps per step)")
+    value = total * len(times) / sum(times)
+    sample = f"the whole batch every step: {len(specs)} instances, {total} integration steps, time evolution and state"
     return {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded tone fields)",
         "impl": "reference",
-        "config": {"workload": "uneven batch: 1024 instances (bounded sample per step)", "threads": threads},
+        "config": {"workload": "uneven batch: 1024 instances, 70% spin-1/2 analytic / 30% spin-1 Lie-Trotter(24), "
+                               "durations log-uniform 10us-10ms, dt_int 10ns, dt_out 1us, 8 tones per axis, "
+                               "Magnus CF4, rotating frame", "integration_steps": total, "threads": threads},
         "cpu_baseline": {"value": value, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -457,6 +461,7 @@ def bench_serving(args):
                      "requests_per_launch_mean": float(np.mean([n for n, _, _, _ in srv.launch_log]))})
         out["rates"][str(int(rate))] = summ
         print(json.dumps({"rate": rate, **summ}), file=sys.stderr, flush=True)
+        del srv, done
     return out
 
 
@@ -476,11 +481,18 @@ def _event_time(fn, reps=3):
     return best
 
 
+def _err_summary(a, b):
+    """Final-state error of each member (max |difference| of state[N-1]): p50 / p99 / max over members."""
+    e = np.array([np.abs(x - y).max() if x.size else 0.0 for x, y in zip(a.final_states(), b.final_states())])
+    return {"members": int(e.size), "p50": float(np.median(e)), "p99": float(np.percentile(e, 99)),
+            "max": float(e.max()), "tolerance": 1e-6}
+
+
 def bench_configs(args):
-    """The drop-in on the other reference workloads (plain FP64, and FP32-bulk where it applies):
-    Larmor precession (spin half, 200,000 output steps), the spin-one detuned Rabi sweep (64 detunings,
-    Lie-Trotter 28 squarings) and the spin-half Gaussian-pulse ensemble (4096 members)."""
-    import math
+    """The drop-in on the other reference workloads, timed with CUDA events: Larmor precession (one
+    evaluate(), spin half, 200,000 output steps), the spin-one detuned Rabi sweep (64 detunings,
+    Lie-Trotter 28 squarings, 10 ms) and the spin-half Gaussian-pulse ensemble (4096 members, 1 ms),
+    each as plain FP64 and, for the sweeps, FP32-bulk with its per-member final-state error."""
     import torch
     import spinsim_b200 as ss
     from spinsim_b200.batch import Batch, Instance
@@ -496,10 +508,11 @@ def bench_configs(args):
                  ss.ExponentiationMethod.LIE_TROTTER, True, 28)
     t2 = time.perf_counter()
     out["simulator_setup_s"] = {"first": t1 - t0, "same_field_again": t2 - t1}
-    # Larmor: one evaluate() through the drop-in API (FP64)
+    # Larmor: one evaluate() through the drop-in API (FP64), outputs copied to the host
     sim = ss.Simulator(F.larmor, ss.SpinQuantumNumber.HALF)
-    t = _event_time(lambda: sim.evaluate(0, 100e-3, 100e-9, 500e-9, ss.SpinQuantumNumber.HALF.plus_x))
-    out["configs"]["larmor_fp64"] = {"steps": 1_000_000, "seconds": t, "steps_per_s": 1e6 / t}
+    t = _event_time(lambda: sim.evaluate(0, 100e-3, 100e-9, 500e-9, ss.SpinQuantumNumber.HALF.plus_x).state)
+    out["configs"]["larmor_fp64"] = {"steps": 1_000_000, "seconds": t, "steps_per_s": 1e6 / t,
+                                     "api": "Simulator.evaluate (results read on the host)"}
     # detuned spin-one Rabi sweep: 64 instances of one user field
     deltas = np.random.default_rng(seed=1).uniform(-5e3, 5e3, 64)
     insts = [Instance(ss.SpinQuantumNumber.ONE, 0, 10e-3, 10e-9, 100e-9, ss.SpinQuantumNumber.ONE.plus_z, [d])
@@ -512,8 +525,7 @@ def bench_configs(args):
         res[prec.name] = b
         out["configs"][f"detuned_rabi_{prec.name.lower()}"] = {"steps": b.total_steps, "seconds": tt,
                                                               "steps_per_s": b.total_steps / tt}
-    e = np.array([np.abs(x - y).max() for x, y in zip(res["FP32_BULK"].final_states(), res["FP64"].final_states())])
-    out["configs"]["detuned_rabi_fp32_bulk"]["state_err_max"] = float(e.max())
+    out["configs"]["detuned_rabi_fp32_bulk"]["state_err"] = _err_summary(res["FP32_BULK"], res["FP64"])
     # Gaussian-pulse ensemble: 4096 members
     members = np.random.default_rng(seed=2).normal(0.0, 500.0, 4096)
     insts = [Instance(ss.SpinQuantumNumber.HALF, 0, 1e-3, 20e-9, 1e-6, ss.SpinQuantumNumber.HALF.plus_z, [m])
@@ -525,10 +537,8 @@ def bench_configs(args):
         res[prec.name] = b
         out["configs"][f"gaussian_ensemble_{prec.name.lower()}"] = {"steps": b.total_steps, "seconds": tt,
                                                                    "steps_per_s": b.total_steps / tt}
-    e = np.array([np.abs(x - y).max() for x, y in zip(res["FP32_BULK"].final_states(), res["FP64"].final_states())])
-    out["configs"]["gaussian_ensemble_fp32_bulk"].update({"state_err_max": float(e.max()),
-                                                          "state_err_p50": float(np.median(e))})
-    _ = math
+    out["configs"]["gaussian_ensemble_fp32_bulk"]["state_err"] = _err_summary(res["FP32_BULK"], res["FP64"])
+    torch.cuda.synchronize()
     return out
 
 
@@ -557,6 +567,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-workloads", action="store_true",
+                    help="skip the other reference workloads and the serving sweep in the main line")
+    ap.add_argument("--line-rates", default="1000,10000,50000", help="serving rates in the main line")
+    ap.add_argument("--line-requests", type=int, default=2000, help="serving requests per rate in the main line")
     ap.add_argument("--workload", default="batch", choices=["batch", "serving", "configs", "profile"])
     ap.add_argument("--profile-size", default="small", choices=["small", "full"])
     ap.add_argument("--precision", default="fp32_bulk", choices=["fp32_bulk", "fp64"])
@@ -595,6 +609,13 @@ def main():
             print(json.dumps(bench_configs(args)), flush=True)
         return
     out, specs = bench_ours(args, world, rank)
+    if rank == 0 and world == 1 and not args.no_extra_workloads:
+        # the other reference workloads and a short serving sweep, in the line the driver records
+        cfg = bench_configs(args)
+        out["reference_workloads"] = {"simulator_setup_s": cfg["simulator_setup_s"], **cfg["configs"]}
+        sweep = argparse.Namespace(**{**vars(args), "rates": args.line_rates, "requests": args.line_requests,
+                                      "hbm_budget_gb": 8.0, "max_registers": 0})
+        out["serving"] = bench_serving(sweep)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         steps, el, frac = cpu_sample(specs, seconds_target=10.0, n_threads=host_threads())

@@ -11,8 +11,15 @@
  *  - Array arguments named *_dev are device pointers (any allocator).  Complex arrays are interleaved
  *    (re, im) doubles, numpy complex128 layout.  Output layouts match the reference's numpy outputs:
  *      time[N] f64, time_evolution U[N][d][d] c128, state[N][d] c128, spin[N][3] f64.
- *  - `stream` is a cudaStream_t (NULL = legacy default stream).  All work is stream-ordered; nothing
- *    synchronises the host except spinsim_plan_create (module load).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  All work is stream-ordered.  The
+ *    single-instance entry points (spinsim_evaluate, spinsim_time_evolution, spinsim_state,
+ *    spinsim_state_static, spinsim_piece_*) and spinsim_batch_launch only launch kernels: their
+ *    descriptors travel as launch arguments and are written into the workspace on the device, so
+ *    they never wait for the stream and can be captured into a CUDA graph (host arrays such as psi0
+ *    are read during the call).  Host waits: spinsim_plan_create (module load; with a user field,
+ *    the link), spinsim_batch_prepare (copies from pageable host memory, which wait for the stream;
+ *    spinsim_batch_prepare_staged copies from the caller's page-locked staging instead), and the
+ *    first spinsim_state_static call on a device (it looks up the library's scratch array).
  *  - The library allocates no device memory on the evaluation path.  Scratch comes from the caller's
  *    workspace, sized by the *_workspace_size queries (256-byte aligned start required).
  */
@@ -159,6 +166,17 @@ int spinsim_evaluate(const spinsim_plan* plan, const spinsim_field* field, doubl
                      int64_t n_out, const double* psi0, double* time_dev, double* u_dev, double* state_dev,
                      double* spin_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
 
+/* spinsim_evaluate plus, for an FP32-bulk plan, the scale of its rounding error: step_norms_dev[i]
+ * receives, for output step i, the sum over its fine steps of |g|^2, g the step generators rounded
+ * to FP32 (the reference has no FP32 form; its results carry no error statement).  The FP32 rounding
+ * errors of the steps are independent, so the final state's error against the FP64 form is of order
+ * 2^-24 sqrt(sum over all steps of |g|^2); spinsim_b200.Results.error_estimate states it.
+ * step_norms_dev may be NULL; an FP64 plan does not write it. */
+int spinsim_evaluate_with_norms(const spinsim_plan* plan, const spinsim_field* field, double t0, double dt_int,
+                                double dt_out, int64_t n_out, const double* psi0, double* time_dev, double* u_dev,
+                                double* state_dev, double* spin_dev, float* step_norms_dev, void* workspace_dev,
+                                size_t workspace_bytes, void* stream);
+
 /* get_time_evolution alone (I:855-896): writes time_dev[N] and u_dev[N][d][d]. */
 int spinsim_time_evolution(const spinsim_plan* plan, const spinsim_field* field, double t0, double dt_int,
                            double dt_out, int64_t n_out, double* time_dev, double* u_dev, void* workspace_dev,
@@ -252,6 +270,10 @@ int spinsim_batch_prepare_staged(const spinsim_plan* plan, const spinsim_instanc
                                  spinsim_batch** out);
 int spinsim_batch_launch(const spinsim_batch* batch, double* time_dev, double* u_dev, double* state_dev,
                          double* spin_dev, void* stream);
+
+/* Batches with an FP32-bulk plan: later launches write step_norms_dev[i] for every output step i of
+ * the flat arrays (instances at their out_offset), as spinsim_evaluate_with_norms does; NULL stops it. */
+int spinsim_batch_set_step_norms(spinsim_batch* batch, float* step_norms_dev);
 
 /* The launch shape a prepared batch runs with (no counterpart in the reference): its tile queue,
  * the output steps per tile, the lanes per output step, and the state scan's tiles. */

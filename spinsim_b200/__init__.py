@@ -102,10 +102,64 @@ class Device(Enum):
 
 class Precision(Enum):
     """Arithmetic of the time-evolution kernel.  ``FP64``: the reference's arithmetic in double
-    precision.  ``FP32_BULK``: single precision for the per-step exponentials, double precision for
-    fields, phases and every product across steps (batched form)."""
+    precision.  ``FP32_BULK``: single precision for the per-step generators and exponentials, double
+    precision for fields, phases and every product across steps (batched form); its results state
+    their error against the FP64 form (``Results.error_estimate``)."""
     FP64 = 0
     FP32_BULK = 1
+
+
+# Error statement of FP32-bulk results against the FP64 form.  Every fine step keeps the linear part
+# of its exponential, -i g.J with g the step generator, in FP64; only its O(|g|^2) remainder (and the
+# Magnus commutator, the quadratic part of the CF4 product) is computed in FP32, so a step's FP32
+# rounding error is at most about 2^-24 |g|^2 (four times that for the sincos branch at |g| > 1/2;
+# twice for spin one, whose operator is the spin-one image of an SU(2) element).  Summed over the
+# steps without any cancellation this gives ERROR_KAPPA[d] 2^-24 sum |g|^2, a bound that holds even
+# when the rounding errors of consecutive steps repeat (slowly varying fields); the kernels accumulate
+# sum |g|^2 on the device (step norms).  Added to it: the FP64 form's Lie-Trotter approximant differs
+# from the exact exponential the FP32-bulk form applies by at most |g|^2 / 4^h per step (h = number of
+# squarings / 2; spin one, and spin half when Lie-Trotter is chosen); tone instances that took the
+# one-exponential Magnus step differ from CF4 by at most MAGNUS_PER_STEP theta^5 per step; and both
+# forms round in FP64, FP64_PER_STEP per step.  The GPU tests check the statement against the
+# measured error on every member of the Gaussian-pulse ensemble (4096 members), the uneven
+# 1024-instance tone batch and the spin-one detuned Rabi sweep.
+FP32_UNIT = 2.0 ** -24
+ERROR_KAPPA = {2: 4.0, 3: 8.0}
+MAGNUS_PER_STEP = 3e-10
+MAGNUS_THETA = 0.1
+FP64_PER_STEP = 2.0 ** -47
+
+
+def bulk_error_estimate(sum_sq, dim, method_bound=0.0, steps=0, lie_trotter_hypercubes=None):
+    """Stated error of an FP32-bulk result against the FP64 form, from the sum over its steps of |g|^2
+    (``sum_sq``), its spin dimension, the Magnus step's bound, its number of fine steps and, when the
+    FP64 form uses Lie-Trotter, its number of hypercubes h (number of squarings / 2)."""
+    sum_sq = max(float(sum_sq), 0.0)
+    err = ERROR_KAPPA[int(dim)] * FP32_UNIT * sum_sq + float(method_bound) + FP64_PER_STEP * float(steps)
+    if lie_trotter_hypercubes is not None:
+        err += sum_sq / 4.0 ** int(lie_trotter_hypercubes)
+    return err
+
+
+def magnus_method_bound(field, time_step_integration, steps):
+    """Bound on the one-exponential Magnus step's difference from CF4 for a tone field instance on the
+    tensor-path kernel (zero when the kernel keeps CF4: theta = h (|B|max + w_max) above MAGNUS_THETA,
+    or any other field)."""
+    if not isinstance(field, ToneField):
+        return 0.0
+    bsq, wmax = 0.0, 0.0
+    for c in range(3):
+        tones = field.tones.get(c)
+        bc = abs(float(field.bias[c]))
+        if tones is not None and len(tones):
+            t = np.asarray(tones, np.float64).reshape(-1, 3)
+            if t.shape[0] > 8:  # more tones than the tensor path takes: the per-interval CF4 path
+                return 0.0
+            bc += float(np.abs(t[:, 1]).sum())
+            wmax = max(wmax, float(np.abs(t[:, 0]).max()))
+        bsq += bc * bc
+    theta = float(time_step_integration) * (math.sqrt(bsq) + wmax)
+    return MAGNUS_PER_STEP * theta ** 5 * steps if theta <= MAGNUS_THETA else 0.0
 
 
 _INTEGRATION_CODE = {IntegrationMethod.MAGNUS_CF4: 0, IntegrationMethod.EULER: 1, IntegrationMethod.HEUN: 2}
@@ -125,12 +179,25 @@ class Results:
 
     _ARRAYS = ("time", "time_evolution", "state", "spin")
 
-    def __init__(self, time, time_evolution, state, spin_calculator=None, *, spin=None, keep=None):
+    def __init__(self, time, time_evolution, state, spin_calculator=None, *, spin=None, keep=None, error=None):
         self.__dict__["_dev"] = {"time": time, "time_evolution": time_evolution, "state": state}
         if spin is not None:
             self.__dict__["_dev"]["spin"] = spin
         self.__dict__["spin_calculator"] = spin_calculator
         self.__dict__["_keep"] = keep
+        self.__dict__["_error"] = error
+
+    @property
+    def error_estimate(self):
+        """Stated error of ``state`` against the FP64 form (max over entries and output steps of the
+        difference; the FP64 form itself matches the reference to 1e-10): 0.0 for FP64 results, the
+        FP32-bulk error statement (``bulk_error_estimate``) for FP32-bulk results, None when unknown
+        (results built from host arrays)."""
+        err = self.__dict__["_error"]
+        if callable(err):
+            err = err()
+            self.__dict__["_error"] = err
+        return err
 
     @property
     def device_arrays(self):
@@ -297,6 +364,13 @@ class Simulator:
         _lib.check(self._lib.spinsim_plan_get_info(self._plan, ctypes.byref(info)))
         return {k: getattr(info, k) for k, _ in _lib.PlanInfo._fields_}
 
+    def _lie_trotter_hypercubes(self):
+        """h = ceil(number_of_squares / 2) when this simulator's FP64 form uses Lie-Trotter, else None."""
+        d = self.spin_quantum_number.dimension
+        if d == 3 or self.exponentiation_method == ExponentiationMethod.LIE_TROTTER:
+            return (int(self.number_of_squares) + 1) // 2
+        return None
+
     def _field_struct(self, sweep_dev):
         if self._builtin is not None:
             return self._builtin[0]
@@ -338,11 +412,25 @@ class Simulator:
         ws = torch.empty(max(ws_bytes, 256), dtype=torch.uint8, device=dev)
         field = self._field_struct(sweep)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(self._lib.spinsim_evaluate(
-            self._plan, ctypes.byref(field), float(time_start), float(dt_int), float(time_step_output), n,
-            psi0.ctypes.data_as(ctypes.c_void_p), time.data_ptr(), u.data_ptr(), state.data_ptr(), spin.data_ptr(),
-            ws.data_ptr(), ws.numel(), stream))
-        return Results(time, u, state, self.spin_calculator, spin=spin, keep=(sweep, ws, self._builtin))
+        if self.precision == Precision.FP32_BULK:
+            norms = torch.zeros(max(n, 1), dtype=torch.float32, device=dev)
+            _lib.check(self._lib.spinsim_evaluate_with_norms(
+                self._plan, ctypes.byref(field), float(time_start), float(dt_int), float(time_step_output), n,
+                psi0.ctypes.data_as(ctypes.c_void_p), time.data_ptr(), u.data_ptr(), state.data_ptr(),
+                spin.data_ptr(), norms.data_ptr(), ws.data_ptr(), ws.numel(), stream))
+            steps = n * int(math.floor(float(time_step_output) / float(dt_int) + 0.5))
+            bound = magnus_method_bound(self.get_field, dt_int, steps)
+            lt = self._lie_trotter_hypercubes()
+
+            def error():
+                return bulk_error_estimate(norms[:n].double().sum().item(), d, bound, steps, lt)
+        else:
+            _lib.check(self._lib.spinsim_evaluate(
+                self._plan, ctypes.byref(field), float(time_start), float(dt_int), float(time_step_output), n,
+                psi0.ctypes.data_as(ctypes.c_void_p), time.data_ptr(), u.data_ptr(), state.data_ptr(),
+                spin.data_ptr(), ws.data_ptr(), ws.numel(), stream))
+            error = 0.0
+        return Results(time, u, state, self.spin_calculator, spin=spin, keep=(sweep, ws, self._builtin), error=error)
 
     def spin_calculator(self, state):
         """get_spin / spin_calculator (I:899-988): Bloch vector of a state series, on the device."""

@@ -79,6 +79,9 @@ _SIGNATURES = [
     ("spinsim_evaluate", ctypes.c_int,
      [c_vp, ctypes.POINTER(Field), c_dbl, c_dbl, c_dbl, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_size_t,
       c_vp]),
+    ("spinsim_evaluate_with_norms", ctypes.c_int,
+     [c_vp, ctypes.POINTER(Field), c_dbl, c_dbl, c_dbl, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+      ctypes.c_size_t, c_vp]),
     ("spinsim_time_evolution", ctypes.c_int,
      [c_vp, ctypes.POINTER(Field), c_dbl, c_dbl, c_dbl, c_i64, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]),
     ("spinsim_state_workspace_size", ctypes.c_size_t, [c_i32, c_i64]),
@@ -101,6 +104,7 @@ _SIGNATURES = [
     ("spinsim_batch_launch", ctypes.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     ("spinsim_batch_destroy", ctypes.c_int, [c_vp]),
     ("spinsim_batch_get_info", ctypes.c_int, [c_vp, ctypes.POINTER(BatchInfo)]),
+    ("spinsim_batch_set_step_norms", ctypes.c_int, [c_vp, c_vp]),
     ("spinsim_fma_peak", ctypes.c_int, [c_i32, ctypes.POINTER(c_dbl), c_vp]),
     ("spinsim_state_static_max_steps", c_i64, []),
     ("spinsim_state_static", ctypes.c_int, [c_i32, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp]),

@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _lib
 from . import (BuiltinField, ExponentiationMethod, IntegrationMethod, Precision, Results, SpinQuantumNumber,
-               _INTEGRATION_CODE, _cuda_device)
+               _INTEGRATION_CODE, _cuda_device, bulk_error_estimate, magnus_method_bound)
 
 
 @dataclass
@@ -165,6 +165,9 @@ class Batch:
         # one device allocation, 256-byte aligned pieces
         pieces = {"time": 8 * max(1, out_off), "u": 8 * max(2, u_off), "state": 8 * max(2, st_off),
                   "spin": 24 * max(1, out_off), "workspace": ws_bytes, "fields": 8 * field_doubles}
+        self.precision = Precision(precision)
+        if self.precision == Precision.FP32_BULK:  # per output step: sum of |g|^2 (the error statement)
+            pieces["norms"] = 4 * max(1, out_off)
         offsets, total = {}, 0
         for name, nbytes in pieces.items():
             offsets[name] = total
@@ -226,6 +229,12 @@ class Batch:
         self._staging = staging
         self._handle = handle
         self._graph = None
+        self._variant = int(variant)
+        self._get_field = get_field
+        self._hypercubes = (int(number_of_squares) + 1) // 2
+        self._lt_half = exponentiation_half == ExponentiationMethod.LIE_TROTTER
+        if "norms" in self._ptr:
+            _lib.check(lib.spinsim_batch_set_step_norms(handle, self._ptr["norms"]))
 
     def run(self, stream=None, with_state=True, with_spin=True):
         """Launch the batch (time evolution + state scan + spin) on ``stream`` (default: current)."""
@@ -351,7 +360,44 @@ class Batch:
         u = self.u[u_off // 2:u_off // 2 + n_out * d * d].view(n_out, d, d)
         st = self.state[st_off // 2:st_off // 2 + n_out * d].view(n_out, d)
         sp = self.spin[out_off:out_off + n_out]
-        return Results(time, u, st, None, spin=sp, keep=keep)
+        error = 0.0
+        if self.precision == Precision.FP32_BULK:
+            norms = self._piece("norms", __import__("torch").float32)
+            terms = self._error_terms(k)
+
+            def error():
+                return bulk_error_estimate(norms[out_off:out_off + n_out].double().sum().item(), d, *terms)
+        return Results(time, u, st, None, spin=sp, keep=keep, error=error)
+
+    def _error_terms(self, k):
+        """(Magnus bound, fine steps, Lie-Trotter hypercubes or None) of instance k's error statement."""
+        rec = self._inst_np[k]
+        steps = int(rec["n_out"]) * int(rec["n_fine"])
+        lt = self._hypercubes if (int(rec["dim"]) == 3 or self._lt_half) else None
+        return self._method_bound(k), steps, lt
+
+    def _method_bound(self, k):
+        inst = self.instances[k]
+        if self._variant != 0 or self._get_field is not None:
+            return 0.0
+        rec = self._inst_np[k]
+        return magnus_method_bound(inst.field, float(rec["dt_int"]), int(rec["n_out"]) * int(rec["n_fine"]))
+
+    def error_estimates(self):
+        """The stated error of every instance's state against the FP64 form (numpy, one per instance):
+        0 for an FP64 batch; for FP32-bulk the error statement from the step norms the launch wrote
+        (one device reduction and one copy for the whole batch)."""
+        import torch
+        n = len(self.instances)
+        if self.precision != Precision.FP32_BULK:
+            return np.zeros(n)
+        rec = self._inst_np
+        norms = self._piece("norms", torch.float32)[:max(1, self.n_intervals)].double()
+        csum = torch.cat([torch.zeros(1, dtype=torch.float64, device=norms.device), torch.cumsum(norms, 0)])
+        lo = torch.from_numpy(rec["out_offset"].astype(np.int64)).to(norms.device)
+        hi = lo + torch.from_numpy(rec["n_out"].astype(np.int64)).to(norms.device)
+        sums = (csum[hi] - csum[lo]).cpu().numpy()
+        return np.array([bulk_error_estimate(sums[k], rec["dim"][k], *self._error_terms(k)) for k in range(n)])
 
     def final_states(self):
         """state[N-1] of every instance as a list of numpy arrays (gathered on the device, so only

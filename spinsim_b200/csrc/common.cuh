@@ -100,6 +100,8 @@ struct EvolveArgs {
     int32_t* tile_counter;   // null: one tile per warp (per CTA on the tensor path) of the grid, no queue
     double* time;            // [sum N]
     double* u;               // complex [sum N * d * d]; instance i starts at u_offset doubles
+    float* step_norms;       // FP32-bulk: per output step, the sum over its fine steps of |g|^2 (the squared
+                             // norms of the generators rounded to FP32); null: not written
 };
 
 // ------------------------------------------------------------------ FP32-bulk tone synthesis

@@ -3,11 +3,14 @@
 // Precision split (errors are stated against the FP64 path, which matches the reference):
 //   FP64  sample times, the rotating-frame phase (a phasor recurrence per interval), field samples
 //         (tones by FP64 phasor recurrences), the frame transform, the CF4 generator combinations,
-//         and the product of steps within the output interval.
-//   FP32  the per-step exponentials in residual form exp(A) - 1, and the product of the two CF4
-//         exponentials of a step.  Only quantities that are recomputed every step are rounded to
-//         FP32, so FP32 rounding errors do not correlate from step to step; constants and
-//         recurrences are never held in FP32.
+//         the linear part of every step's exponential (exp(A) - 1 = A + ..., A from the FP64
+//         generators), and the product of steps within the output interval.
+//   FP32  the rest of each exponential (its O(|A|^2) part), the product of the two CF4
+//         exponentials of a step (its quadratic part) and the Magnus commutator (tensor-path
+//         kernel).  So every FP32 rounding error of a step is O(2^-24 |g|^2) in the step generator
+//         g: a step's first-order term, the one that adds up over 10^6 steps even when the field
+//         varies slowly and its roundings repeat, is never rounded to FP32.  The kernels accumulate
+//         sum |g|^2 per output step (the error statement, spinsim_b200.bulk_error_estimate).
 //
 // Exponentials.  Spin half: the exact SU(2) exponential exp(-i g.sigma/2) - 1 from even power
 // series in r^2 = |g|^2 (no square root or division) for r <= 1/2, sincos otherwise.  Spin one with
@@ -53,46 +56,43 @@ struct Su2d {
     c64 am1, beta;
 };
 
-// exp(-i (x sigma_x + y sigma_y + z sigma_z) / 2) - 1 as (alpha - 1, beta); the reference's analytic
-// spin-half exponential (I:1618-1642) is the same element.
-SS_D Su2f su2_exp(float x, float y, float z) {
+// The FP32 remainder of exp(-i g.sigma/2) - 1 beyond its linear part -i g.sigma/2 (which the caller
+// takes in FP64): alpha - 1 = -i gz/2 + [c - i gz s'],  beta = (gy - i gx)/2 + [(gy - i gx) s'],
+// c = cos(r/2) - 1, s' = sin(r/2)/r - 1/2, r = |g|: both O(r^2), from even series for r <= 1/2.
+SS_D Su2f su2_exp_rest(float x, float y, float z) {
     const float r2 = fmaf(x, x, fmaf(y, y, z * z));
-    float c, s;  // c = cos(r/2) - 1, s = sin(r/2) / r
+    float c, sp;
     if (r2 <= 0.25f) {
         c = r2 * (-0.125f + r2 * (1.0f / 384.0f + r2 * (-1.0f / 46080.0f + r2 * (1.0f / 10321920.0f -
                                                                             r2 * (1.0f / 3715891200.0f)))));
-        s = 0.5f + r2 * (-1.0f / 48.0f + r2 * (1.0f / 3840.0f + r2 * (-1.0f / 645120.0f + r2 * (1.0f / 185794560.0f))));
+        sp = r2 * (-1.0f / 48.0f + r2 * (1.0f / 3840.0f + r2 * (-1.0f / 645120.0f + r2 * (1.0f / 185794560.0f))));
     } else {
         const float r = sqrtf(r2);
         float s4, c4;
         sincosf(0.25f * r, &s4, &c4);
         c = -2.0f * s4 * s4;
-        s = 2.0f * s4 * c4 / r;
+        sp = 2.0f * s4 * c4 / r - 0.5f;
     }
     Su2f e;
-    e.am1 = c32{c, -z * s};
-    e.beta = c32{y * s, -x * s};
+    e.am1 = c32{c, -z * sp};
+    e.beta = c32{y * sp, -x * sp};
     return e;
 }
 
-// b * a (a first) in residual form
-SS_D Su2f su2_mul(const Su2f& b, const Su2f& a) {
-    // alpha = ab_a - conj(bb) ba; beta = bb aa + conj(ab) ba
+// The whole element in FP32 (linear part rounded) from its remainder: for quadratic terms only.
+SS_D Su2f su2_full(float x, float y, float z, const Su2f& rest) {
+    return Su2f{c32{rest.am1.re, fmaf(-0.5f, z, rest.am1.im)}, c32{fmaf(0.5f, y, rest.beta.re), fmaf(-0.5f, x, rest.beta.im)}};
+}
+
+// The quadratic part b a of (1 + b)(1 + a) - 1 = a + b + b a (b later).
+SS_D Su2f su2_prod(const Su2f& b, const Su2f& a) {
     Su2f o;
-    const c32 cross = conjf(b.beta) * a.beta;
-    o.am1 = (b.am1 * a.am1 + (b.am1 + a.am1)) - cross;
-    o.beta = (b.beta * a.am1 + b.beta) + (conjf(b.am1) * a.beta + a.beta);
+    o.am1 = b.am1 * a.am1 - conjf(b.beta) * a.beta;
+    o.beta = b.beta * a.am1 + conjf(b.am1) * a.beta;
     return o;
 }
 
-SS_D Mat32<2> su2_mat_m1(const Su2f& e) {
-    Mat32<2> m;
-    m.a[0][0] = e.am1;
-    m.a[1][0] = e.beta;
-    m.a[0][1] = c32{-e.beta.re, e.beta.im};  // -conj(beta)
-    m.a[1][1] = conjf(e.am1);
-    return m;
-}
+SS_D Su2f su2_add(const Su2f& a, const Su2f& b) { return Su2f{a.am1 + b.am1, a.beta + b.beta}; }
 
 // Spin-one representation of an FP64 SU(2) element (full matrix, not residual).
 SS_D Mat<3> su2_to_spin_one(const c64& alpha, const c64& beta) {
@@ -173,46 +173,79 @@ SS_D Mat32<3> spin_one_exp_m1(float x, float y, float z, float q) {
     return R;
 }
 
-template <int D>
-SS_D Mat32<D> mul_m1_f(const Mat32<D>& l, const Mat32<D>& r) {  // (l + r) + l r
-    Mat32<D> o;
-#pragma unroll
-    for (int i = 0; i < D; i++)
-#pragma unroll
-        for (int j = 0; j < D; j++) {
-            c32 acc = l.a[i][j] + r.a[i][j];
-#pragma unroll
-            for (int k = 0; k < D; k++) acc = cfmaf(l.a[i][k], r.a[k][j], acc);
-            o.a[i][j] = acc;
-        }
-    return o;
+// A = -i H for H = x Jx + y Jy + z Jz + q Q (spin one, Q = diag(1, -2, 1) / 3), the linear part of
+// exp(A) - 1, in FP64 or FP32.
+template <typename T, typename C>
+SS_D void spin_one_generator_into(T x, T y, T z, T q, C (&a)[3][3]) {
+    const T ir2 = (T)0.70710678118654752440;
+    const T pr = x * ir2, pi = y * ir2;
+    const T h0 = z + q / (T)3, h1 = -q * ((T)2 / (T)3), h2 = -z + q / (T)3;
+    a[0][0] = C{(T)0, -h0};
+    a[1][1] = C{(T)0, -h1};
+    a[2][2] = C{(T)0, -h2};
+    a[1][0] = C{pi, -pr};
+    a[2][1] = C{pi, -pr};
+    a[0][1] = C{-pi, -pr};
+    a[1][2] = C{-pi, -pr};
+    a[2][0] = C{(T)0, (T)0};
+    a[0][2] = C{(T)0, (T)0};
 }
 
-// U <- U + D U with D in FP32 (converted once) and U in FP64.
-template <int D>
-SS_D void apply_m1(Mat<D>& u, const Mat32<D>& dm) {
-    c64 d[D][D];
+// u <- u + (a64 + rest) u: the step's linear part in FP64, its remainder converted from FP32.
+SS_D void apply_split3(Mat<3>& u, const c64 (&a64)[3][3], const Mat32<3>& rest) {
+    c64 d[3][3];
 #pragma unroll
-    for (int i = 0; i < D; i++)
+    for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int k = 0; k < D; k++) d[i][k] = c64{(double)dm.a[i][k].re, (double)dm.a[i][k].im};
-    Mat<D> o;
+        for (int k = 0; k < 3; k++) d[i][k] = c64{a64[i][k].re + (double)rest.a[i][k].re, a64[i][k].im + (double)rest.a[i][k].im};
+    Mat<3> o;
 #pragma unroll
-    for (int i = 0; i < D; i++)
+    for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < D; j++) {
+        for (int j = 0; j < 3; j++) {
             c64 acc = u.a[i][j];
 #pragma unroll
-            for (int k = 0; k < D; k++) acc = cfma(d[i][k], u.a[k][j], acc);
+            for (int k = 0; k < 3; k++) acc = cfma(d[i][k], u.a[k][j], acc);
             o.a[i][j] = acc;
         }
     u = o;
 }
 
-// SU(2) product in FP64: P <- (1 + E) P, with E an FP32 residual element.
-SS_D void su2_apply(Su2d& p, const Su2f& e) {
-    const c64 am1 = c64{(double)e.am1.re, (double)e.am1.im};
-    const c64 b = c64{(double)e.beta.re, (double)e.beta.im};
+// One CF4 step of spin one with a quadratic shift: E = Ea + Eb + Eb Ea with Ea = exp(A(ga)) - 1, its
+// linear part A(ga + gb) in FP64, the rest (series remainders and the product) in FP32.
+SS_D void spin_one_cf4_step(Mat<3>& u, const double* ga, const double* gb, float* nsq) {
+    float a[4], b[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        a[k] = __double2float_rn(ga[k]);
+        b[k] = __double2float_rn(gb[k]);
+        *nsq = fmaf(a[k], a[k], fmaf(b[k], b[k], *nsq));
+    }
+    const Mat32<3> ra = spin_one_exp_m1(a[0], a[1], a[2], a[3]);
+    const Mat32<3> rb = spin_one_exp_m1(b[0], b[1], b[2], b[3]);
+    c32 la[3][3], lb[3][3];
+    spin_one_generator_into<float, c32>(a[0], a[1], a[2], a[3], la);
+    spin_one_generator_into<float, c32>(b[0], b[1], b[2], b[3], lb);
+    Mat32<3> rest;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            c32 acc = (ra.a[i][j] - la[i][j]) + (rb.a[i][j] - lb[i][j]);
+#pragma unroll
+            for (int k = 0; k < 3; k++) acc = cfmaf(rb.a[i][k], ra.a[k][j], acc);
+            rest.a[i][j] = acc;
+        }
+    c64 lin[3][3];
+    spin_one_generator_into<double, c64>(ga[0] + gb[0], ga[1] + gb[1], ga[2] + gb[2], ga[3] + gb[3], lin);
+    apply_split3(u, lin, rest);
+}
+
+// P <- (1 + E) P in FP64 with E = -i g.sigma/2 (g the step's FP64 generator: the linear part, never
+// rounded to FP32) + rest (its FP32 remainder).
+SS_D void su2_apply_split(Su2d& p, double gx, double gy, double gz, const Su2f& rest) {
+    const c64 am1 = c64{(double)rest.am1.re, fma(-0.5, gz, (double)rest.am1.im)};
+    const c64 b = c64{fma(0.5, gy, (double)rest.beta.re), fma(-0.5, gx, (double)rest.beta.im)};
     // alpha' = alpha_e alpha - conj(beta_e) beta ; beta' = beta_e alpha + conj(alpha_e) beta
     const c64 alpha = c64{1.0 + p.am1.re, p.am1.im};
     const c64 na = cfma(am1, alpha, p.am1) - conj(b) * p.beta;  // (alpha - 1) + am1 alpha - conj(b) beta
@@ -221,12 +254,28 @@ SS_D void su2_apply(Su2d& p, const Su2f& e) {
     p.beta = nb;
 }
 
+// One CF4 step as an SU(2) element: E = Ea + Eb + Eb Ea with Ea = exp(-i ga.sigma/2) - 1; its linear
+// part -i (ga + gb).sigma/2 in FP64, the series remainders and the product Eb Ea in FP32.
+SS_D void su2_cf4_step(Su2d& p, const double* ga, const double* gb, float* nsq) {
+    float a[3], b[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        a[c] = __double2float_rn(ga[c]);
+        b[c] = __double2float_rn(gb[c]);
+        *nsq = fmaf(a[c], a[c], fmaf(b[c], b[c], *nsq));
+    }
+    const Su2f ra = su2_exp_rest(a[0], a[1], a[2]);
+    const Su2f rb = su2_exp_rest(b[0], b[1], b[2]);
+    const Su2f prod = su2_prod(su2_full(b[0], b[1], b[2], rb), su2_full(a[0], a[1], a[2], ra));
+    su2_apply_split(p, ga[0] + gb[0], ga[1] + gb[1], ga[2] + gb[2], su2_add(su2_add(ra, rb), prod));
+}
+
 // ---------------------------------------------------------------------------------- generic bulk path
 // One output interval per lane (USER and TABLE fields, and tone fields the synthesis below does not
 // take: spin one with a quadratic shift).
 template <int D, int INTEG, int EXPO, int FIELD>
 SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDesc& f, int64_t index, bool active,
-                     int lane_in_group, double* time_out, double* u_out) {
+                     int lane_in_group, double* time_out, double* u_out, float* norms_out) {
     static_assert(INTEG == INTEG_CF4, "the FP32-bulk form is built for Magnus CF4");
     static_assert(EXPO != EXPO_LIE_TROTTER_8, "the FP32-bulk form has no eight-generator exponential");
     constexpr int L = (D == 2) ? 3 : 4;
@@ -268,8 +317,8 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
 #pragma unroll
     for (int c = 0; c < L; c++) cur[c] = TableCursor{-1, 0.0, 0.0};
 
-    // One step's field samples (FP64) -> frame transform -> CF4 generators rounded to FP32.
-    auto step_generators = [&](float* ga, float* gb) {
+    // One step's field samples (FP64) -> frame transform -> CF4 generators (FP64).
+    auto step_generators = [&](double* ga, double* gb) {
 #pragma unroll
         for (int k = 0; k < L; k++) {
             s0[k] = 0.0;
@@ -291,8 +340,8 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         }
 #pragma unroll
         for (int k = 0; k < L; k++) {
-            ga[k] = __double2float_rn(fma(c0, s0[k], c1 * s1[k]));
-            gb[k] = __double2float_rn(fma(c1, s0[k], c0 * s1[k]));
+            ga[k] = fma(c0, s0[k], c1 * s1[k]);
+            gb[k] = fma(c1, s0[k], c0 * s1[k]);
         }
     };
 
@@ -300,21 +349,22 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     // is zero); the interval product is an FP64 SU(2) element.  Software-pipelined: the next step's
     // field samples (independent FP64 work) are issued next to this step's exponentials and product.
     Su2d su2 = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
-    float ga[4] = {0.0f, 0.0f, 0.0f, 0.0f}, gb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    double ga[4] = {0.0, 0.0, 0.0, 0.0}, gb[4] = {0.0, 0.0, 0.0, 0.0};
+    float nsq = 0.0f;  // sum of |g|^2 over this lane's steps (the error statement's scale)
     int j = j0;
     bool pending = false;
     if (j < j1) step_generators(ga, gb);
     for (; j < j1; j++) {
         if constexpr (D == 3) {
-            if (ga[3] != 0.0f || gb[3] != 0.0f) {
+            if (ga[3] != 0.0 || gb[3] != 0.0) {
                 pending = true;
                 break;
             }
         }
-        float na[4] = {0.0f, 0.0f, 0.0f, 0.0f}, nb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        double na[4] = {0.0, 0.0, 0.0, 0.0}, nb[4] = {0.0, 0.0, 0.0, 0.0};
         t_fine += dt;
         if (j + 1 < j1) step_generators(na, nb);
-        su2_apply(su2, su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2])));
+        su2_cf4_step(su2, ga, gb, &nsq);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             ga[k] = na[k];
@@ -341,9 +391,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             for (; j < j1; j++) {
                 if (!first) step_generators(ga, gb);
                 first = false;
-                const Mat32<3> ea = spin_one_exp_m1(ga[0], ga[1], ga[2], ga[3]);
-                const Mat32<3> eb = spin_one_exp_m1(gb[0], gb[1], gb[2], gb[3]);
-                apply_m1<3>(u, mul_m1_f<3>(eb, ea));
+                spin_one_cf4_step(u, ga, gb, &nsq);
                 t_fine += dt;
             }
         }
@@ -351,6 +399,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
 
     for (int s = 1; s < lanes; s <<= 1) {
         const Mat<D> later = shfl_down_mat(u, s);
+        nsq += __shfl_down_sync(0xffffffffu, nsq, s);
         if ((lane_in_group & (2 * s - 1)) == 0) u = matmul(later, u);
     }
     if (!active || lane_in_group != 0) return;
@@ -365,6 +414,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         }
     }
     time_out[index] = t_c;
+    if (norms_out != nullptr) norms_out[index] = nsq;
     double2* dst = reinterpret_cast<double2*>(u_out) + index * (D * D);
 #pragma unroll
     for (int i = 0; i < D; i++)
@@ -391,7 +441,7 @@ SS_D bool tones_have_quadratic_shift(const FieldDesc& f) { return f.bias[3] != 0
 
 template <int D, int EXPO>
 SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const FieldDesc& f, const Tile& tile,
-                            double* time_out, double* u_out) {
+                            double* time_out, double* u_out, float* norms_out) {
     constexpr int NI = kSynthIntervals;
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lane = threadIdx.x & 31;
@@ -461,8 +511,12 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
     }
 
     Su2d su2[NI];
+    float nsq[NI];
 #pragma unroll
-    for (int i = 0; i < NI; i++) su2[i] = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
+    for (int i = 0; i < NI; i++) {
+        su2[i] = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
+        nsq[i] = 0.0f;
+    }
     for (int j = 0; j < K; j++) {
         // publish G^i U, G^i V of step j
         if (lane < kToneSlots) {
@@ -541,13 +595,13 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
                 sb[i][2] -= (double)P * rw[i];
                 W[i] = Wn;
             }
-            float ga[3], gb[3];
+            double ga[3], gb[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                ga[c] = __double2float_rn(fma(c0, sa[i][c], c1 * sb[i][c]));
-                gb[c] = __double2float_rn(fma(c1, sa[i][c], c0 * sb[i][c]));
+                ga[c] = fma(c0, sa[i][c], c1 * sb[i][c]);
+                gb[c] = fma(c1, sa[i][c], c0 * sb[i][c]);
             }
-            su2_apply(su2[i], su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2])));
+            su2_cf4_step(su2[i], ga, gb, &nsq[i]);
         }
     }
     __syncwarp();  // the shared slots are reused by the warp's next tile
@@ -576,6 +630,7 @@ SS_D void intervals32_synth(const MethodConfig& m, const Instance& inst, const F
             }
         }
         time_out[index[i]] = t_c[i];
+        if (norms_out != nullptr) norms_out[index[i]] = nsq[i];
         double2* dst = reinterpret_cast<double2*>(u_out) + index[i] * (D * D);
 #pragma unroll
         for (int r = 0; r < D; r++)

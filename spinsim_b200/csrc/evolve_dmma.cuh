@@ -32,10 +32,10 @@
 // (the commutator [A2, A1] of A = -i b.J is -i (b2 x b1).J; Blanes, Casas and Ros, BIT 40 (2000)),
 // is the same map to O(h^5): one SU(2) exponential per step.  A tile takes it when the step is small
 // against the field, theta = h (|B|max + w_max) <= kMagnusTheta, and CF4 otherwise.  The frame
-// transform and the sum and difference of the samples stay in FP64; g and the commutator are formed
-// in FP32 (g rounded once per step), the exponential is FP32 and the interval product FP64
-// (su2_apply).  On the benchmark's longest instances (theta = 0.07) the two compositions agree to
-// 1e-11 in the final state, far below the FP32 rounding of g.  Instances with more than kBulkTones
+// transform, the sum and difference of the samples and the exponential's linear part stay in FP64;
+// the commutator and the exponential's O(|g|^2) remainder are FP32, the interval product FP64
+// (su2_apply_split).  On the benchmark's longest instances (theta = 0.07) the two compositions agree
+// to 1e-11 in the final state.  Instances with more than kBulkTones
 // tones on a channel, or spin one with a quadratic shift, take the per-interval path (interval32,
 // CF4) inside the same kernel.
 #pragma once
@@ -102,7 +102,7 @@ SS_D bool dmma_eligible(const FieldDesc& f, int dim) {
 
 template <int D>
 SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc& f, const Tile& tile, DmmaShared& sh,
-                    double* time_out, double* u_out) {
+                    double* time_out, double* u_out, float* norms_out) {
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
@@ -250,6 +250,7 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
     // CF4 generators from samples in units of h / 2: h (w0 b1 + w1 b2) = 2 w0 sa + 2 w1 sb
     constexpr double kW0 = (1.5 + kSqrt3) / 3.0, kW1 = (1.5 - kSqrt3) / 3.0;
     Su2d acc = Su2d{c64{0.0, 0.0}, c64{0.0, 0.0}};
+    float nsq = 0.0f;  // sum of |g|^2 over this lane's steps (the error statement's scale)
     const int n_phases = (n_steps + kDmmaPhase - 1) / kDmmaPhase;
     for (int ph = 0; ph < n_phases; ph++) {
         if (ph + 1 < n_phases) fill(ph + 1);
@@ -292,26 +293,34 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
                 }
                 if (magnus) {
                     // g = (h / 2)(b1 + b2) + (sqrt3 h^2 / 12) b2 x b1, with (h / 2) b in sa, sb: the
-                    // commutator term is (sqrt3 / 6) d x g_lin, d = (h / 2)(b2 - b1); g rounded once to FP32.
+                    // linear part g_lin = sa + sb stays FP64; the commutator (sqrt3 / 6) d x g_lin,
+                    // d = (h / 2)(b2 - b1), and the exponential's remainder are FP32.
+                    double gl64[3];
                     float gl[3], dd[3];
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
-                        gl[c] = __double2float_rn(sa[c] + sb[c]);
+                        gl64[c] = sa[c] + sb[c];
+                        gl[c] = __double2float_rn(gl64[c]);
                         dd[c] = __double2float_rn(sb[c] - sa[c]);
                     }
                     constexpr float kComm = 0.28867513459481287f;  // sqrt3 / 6
-                    const float g0 = fmaf(kComm, fmaf(dd[1], gl[2], -dd[2] * gl[1]), gl[0]);
-                    const float g1 = fmaf(kComm, fmaf(dd[2], gl[0], -dd[0] * gl[2]), gl[1]);
-                    const float g2 = fmaf(kComm, fmaf(dd[0], gl[1], -dd[1] * gl[0]), gl[2]);
-                    su2_apply(acc, su2_exp(g0, g1, g2));
-                } else {  // the reference's CF4 (I:655-686): two exponentials, their product in FP32
-                    float ga[3], gb[3];
+                    const float cx = kComm * fmaf(dd[1], gl[2], -dd[2] * gl[1]);
+                    const float cy = kComm * fmaf(dd[2], gl[0], -dd[0] * gl[2]);
+                    const float cz = kComm * fmaf(dd[0], gl[1], -dd[1] * gl[0]);
+                    Su2f rest = su2_exp_rest(gl[0] + cx, gl[1] + cy, gl[2] + cz);
+                    rest.am1.im = fmaf(-0.5f, cz, rest.am1.im);  // the commutator's linear part
+                    rest.beta.re = fmaf(0.5f, cy, rest.beta.re);
+                    rest.beta.im = fmaf(-0.5f, cx, rest.beta.im);
+                    su2_apply_split(acc, gl64[0], gl64[1], gl64[2], rest);
+                    nsq = fmaf(gl[0], gl[0], fmaf(gl[1], gl[1], fmaf(gl[2], gl[2], nsq)));
+                } else {  // the reference's CF4 (I:655-686): two exponentials
+                    double ga[3], gb[3];
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
-                        ga[c] = __double2float_rn(fma(kW0, sa[c], kW1 * sb[c]));
-                        gb[c] = __double2float_rn(fma(kW1, sa[c], kW0 * sb[c]));
+                        ga[c] = fma(kW0, sa[c], kW1 * sb[c]);
+                        gb[c] = fma(kW1, sa[c], kW0 * sb[c]);
                     }
-                    su2_apply(acc, su2_mul(su2_exp(gb[0], gb[1], gb[2]), su2_exp(ga[0], ga[1], ga[2])));
+                    su2_cf4_step(acc, ga, gb, &nsq);
                 }
             }
         }
@@ -322,6 +331,7 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
 #pragma unroll
     for (int sft = 1; sft < kDmmaSegments; sft <<= 1) {
         const Su2d later = shfl_down_su2(acc, sft);
+        nsq += __shfl_down_sync(0xffffffffu, nsq, sft);
         if ((q & (2 * sft - 1)) == 0) acc = su2d_mul(later, acc);
     }
     if (active && q == 0) {
@@ -346,6 +356,7 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
             }
         }
         time_out[idx] = t_c;
+        if (norms_out != nullptr) norms_out[idx] = nsq;
         double2* dst = reinterpret_cast<double2*>(u_out) + idx * (D * D);
 #pragma unroll
         for (int r = 0; r < D; r++)
@@ -379,18 +390,19 @@ SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
         const FieldDesc& f = a.fields[inst.field];
         double* time_out = a.time + inst.out_offset;
         double* u_out = a.u + inst.u_offset;
+        float* norms_out = a.step_norms != nullptr ? a.step_norms + inst.out_offset : nullptr;
         const int dim = (DIMS == 0) ? inst.dim : DIMS;
         if (dmma_eligible(f, dim)) {
-            if (DIMS != 3 && dim == 2) tile_dmma<2>(a.m, inst, f, tile, sh, time_out, u_out);
-            else if (DIMS != 2) tile_dmma<3>(a.m, inst, f, tile, sh, time_out, u_out);
+            if (DIMS != 3 && dim == 2) tile_dmma<2>(a.m, inst, f, tile, sh, time_out, u_out, norms_out);
+            else if (DIMS != 2) tile_dmma<3>(a.m, inst, f, tile, sh, time_out, u_out, norms_out);
         } else if (threadIdx.x < tile.count) {
             // more tones than the products take, or a quadratic shift: one interval per thread
             if (DIMS != 3 && dim == 2)
                 interval32<2, INTEG_CF4, EXPO_ANALYTIC, FIELD_TONES>(a.m, inst, f, tile.first + threadIdx.x, true, 0,
-                                                                     time_out, u_out);
+                                                                     time_out, u_out, norms_out);
             else if (DIMS != 2)
                 interval32<3, INTEG_CF4, EXPO_LIE_TROTTER, FIELD_TONES>(a.m, inst, f, tile.first + threadIdx.x, true, 0,
-                                                                        time_out, u_out);
+                                                                        time_out, u_out, norms_out);
         }
         __syncthreads();  // shared memory and the tile slot are reused by the next tile
         if (a.tile_counter == nullptr) return;

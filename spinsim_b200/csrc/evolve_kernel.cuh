@@ -47,6 +47,7 @@ SS_D void evolve_body(const EvolveArgs& a) {
         const FieldDesc& f = a.fields[inst.field];
         double* time_out = a.time + inst.out_offset;
         double* u_out = a.u + inst.u_offset;
+        float* norms_out = a.step_norms != nullptr ? a.step_norms + inst.out_offset : nullptr;
         const int dim = (DIMS == 0) ? inst.dim : DIMS;
         if constexpr (SYNTH) {
             if (DIMS != 2 && dim == 3 && tones_have_quadratic_shift(f)) {
@@ -55,12 +56,12 @@ SS_D void evolve_body(const EvolveArgs& a) {
                 for (int i = 0; i < kSynthIntervals; i++) {
                     const bool act = lane + 32 * i < tile.count;
                     const int64_t idx = tile.first + (act ? lane + 32 * i : 0);
-                    interval32<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, idx, act, 0, time_out, u_out);
+                    interval32<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, idx, act, 0, time_out, u_out, norms_out);
                 }
             } else if (DIMS != 3 && dim == 2) {
-                intervals32_synth<2, EXPO_H>(a.m, inst, f, tile, time_out, u_out);
+                intervals32_synth<2, EXPO_H>(a.m, inst, f, tile, time_out, u_out, norms_out);
             } else if (DIMS != 2) {
-                intervals32_synth<3, EXPO_O>(a.m, inst, f, tile, time_out, u_out);
+                intervals32_synth<3, EXPO_O>(a.m, inst, f, tile, time_out, u_out, norms_out);
             }
         } else {
             const bool active = group < tile.count;
@@ -69,12 +70,12 @@ SS_D void evolve_body(const EvolveArgs& a) {
                 if constexpr (PREC == PREC_FP64)
                     interval64<2, INTEG, EXPO_H, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
                 else
-                    interval32<2, INTEG, EXPO_H, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
+                    interval32<2, INTEG, EXPO_H, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out, norms_out);
             } else if (DIMS != 2) {
                 if constexpr (PREC == PREC_FP64)
                     interval64<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
                 else
-                    interval32<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out);
+                    interval32<3, INTEG, EXPO_O, FIELD>(a.m, inst, f, index, active, lane_in_group, time_out, u_out, norms_out);
             }
         }
         if (a.tile_counter == nullptr) return;
