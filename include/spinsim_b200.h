@@ -282,6 +282,9 @@ typedef struct {
     int64_t scan_tiles;     /* state-scan tiles (with padding to whole warps) */
     int32_t lanes;          /* lanes per output step */
     int32_t tile_intervals; /* output steps per time-evolution tile */
+    int32_t scan_partials;  /* 1: the time evolution writes the state scan's tile partials (tensor path,
+                               every instance's field on it) and the scan launches no tile products */
+    int32_t reserved;
 } spinsim_batch_info;
 int spinsim_batch_get_info(const spinsim_batch* batch, spinsim_batch_info* info);
 int spinsim_batch_destroy(spinsim_batch* batch);

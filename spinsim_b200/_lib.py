@@ -51,7 +51,8 @@ class PlanInfo(ctypes.Structure):
 
 
 class BatchInfo(ctypes.Structure):
-    _fields_ = [("tiles", c_i64), ("scan_tiles", c_i64), ("lanes", c_i32), ("tile_intervals", c_i32)]
+    _fields_ = [("tiles", c_i64), ("scan_tiles", c_i64), ("lanes", c_i32), ("tile_intervals", c_i32),
+                ("scan_partials", c_i32), ("reserved", c_i32)]
 
 
 class SpinsimError(RuntimeError):

@@ -102,12 +102,29 @@ struct EvolveArgs {
     double* u;               // complex [sum N * d * d]; instance i starts at u_offset doubles
     float* step_norms;       // FP32-bulk: per output step, the sum over its fine steps of |g|^2 (the squared
                              // norms of the generators rounded to FP32); null: not written
+    double* tile_partials;   // tensor path: per scan tile (kScanTile output steps, kScanMat doubles), each
+                             // warp's product of its rows as an SU(2) pair in the lab frame (4 doubles per
+                             // warp, warp after warp); null: not written
+    const int32_t* scan_begin;  // per instance: its first scan tile (null: one instance, tile 0)
 };
+
+// State scan tiles (scan.cuh): consecutive output steps of one instance per tile, and the doubles
+// kept per stored tile operator (3 x 3 complex; spin half uses 8).
+constexpr int kScanTile = 32;
+constexpr int kScanMat = 18;
 
 // ------------------------------------------------------------------ FP32-bulk tone synthesis
 // Shared memory of the FP32-bulk tone kernels (see evolve32.cuh), per warp.
 constexpr int kBulkTones = 8;               // tones per channel (x, y, z) synthesised per warp
 constexpr int kToneSlots = 3 * kBulkTones;  // slot = channel * kBulkTones + tone
+
+// A tone field whose samples the tensor-path kernel forms as products: at most kBulkTones tones per
+// channel and, for spin one, no quadratic shift (other fields take that kernel's per-interval path).
+SS_HD bool tones_on_tensor_path(const FieldDesc& f, int dim) {
+    for (int c = 0; c < 3; c++)
+        if (f.tone_count[c] > kBulkTones) return false;
+    return !(dim == 3 && (f.bias[3] != 0.0 || f.tone_count[3] > 0));
+}
 constexpr int kSynthIntervals = 2;          // output intervals per lane, 32 intervals apart
 // Slot-fastest layouts: a warp's 16-byte stores and loads of one quantity for all slots are
 // contiguous (no bank conflicts); the consumers' reads of one slot are broadcasts.
@@ -210,7 +227,78 @@ SS_HD Mat<D> multiply_m1(const Mat<D>& l, const Mat<D>& r) {
     return o;
 }
 
+// An SU(2) element as its pair (a, b): U = [[a, -conj b], [b, conj a]].
+struct Su2p {
+    c64 a, b;
+};
+
+SS_D Su2p su2p_identity() { return Su2p{c64{1.0, 0.0}, c64{0.0, 0.0}}; }
+
+// x y (x later)
+SS_D Su2p su2p_mul(const Su2p& x, const Su2p& y) {
+    return Su2p{x.a * y.a - conj(x.b) * y.b, cfma(x.b, y.a, conj(x.a) * y.b)};
+}
+
+// Spin-one representation of an SU(2) element (the image of U under the spin-one map).
+SS_D Mat<3> su2_to_spin_one(const c64& alpha, const c64& beta) {
+    constexpr double r2 = 1.4142135623730951;
+    Mat<3> m;
+    const c64 ac = conj(alpha), bc = conj(beta);
+    m.a[0][0] = alpha * alpha;
+    m.a[1][0] = r2 * (alpha * beta);
+    m.a[2][0] = beta * beta;
+    m.a[0][1] = (-r2) * (alpha * bc);
+    m.a[1][1] = c64{alpha.re * alpha.re + alpha.im * alpha.im - beta.re * beta.re - beta.im * beta.im, 0.0};
+    m.a[2][1] = r2 * (ac * beta);
+    m.a[0][2] = bc * bc;
+    m.a[1][2] = (-r2) * (ac * bc);
+    m.a[2][2] = ac * ac;
+    return m;
+}
+
+// The d x d operator of an SU(2) element: itself (spin half) or its spin-one representation.
+template <int D>
+SS_D Mat<D> su2p_to_mat(const Su2p& v) {
+    if constexpr (D == 2) {
+        Mat<2> m;
+        m.a[0][0] = v.a;
+        m.a[1][0] = v.b;
+        m.a[0][1] = c64{-v.b.re, v.b.im};
+        m.a[1][1] = conj(v.a);
+        return m;
+    } else {
+        return su2_to_spin_one(v.a, v.b);
+    }
+}
+
 #ifdef __CUDACC__
+SS_D Su2p shfl_down_su2p(const Su2p& v, int delta) {
+    Su2p o;
+    o.a.re = __shfl_down_sync(0xffffffffu, v.a.re, delta);
+    o.a.im = __shfl_down_sync(0xffffffffu, v.a.im, delta);
+    o.b.re = __shfl_down_sync(0xffffffffu, v.b.re, delta);
+    o.b.im = __shfl_down_sync(0xffffffffu, v.b.im, delta);
+    return o;
+}
+
+SS_D Su2p shfl_up_su2p(const Su2p& v, int delta) {
+    Su2p o;
+    o.a.re = __shfl_up_sync(0xffffffffu, v.a.re, delta);
+    o.a.im = __shfl_up_sync(0xffffffffu, v.a.im, delta);
+    o.b.re = __shfl_up_sync(0xffffffffu, v.b.re, delta);
+    o.b.im = __shfl_up_sync(0xffffffffu, v.b.im, delta);
+    return o;
+}
+
+SS_D Su2p shfl_su2p(const Su2p& v, int src) {
+    Su2p o;
+    o.a.re = __shfl_sync(0xffffffffu, v.a.re, src);
+    o.a.im = __shfl_sync(0xffffffffu, v.a.im, src);
+    o.b.re = __shfl_sync(0xffffffffu, v.b.re, src);
+    o.b.im = __shfl_sync(0xffffffffu, v.b.im, src);
+    return o;
+}
+
 // Warp shuffles of a whole operator (every lane of the warp must take part).
 template <int D>
 __device__ __forceinline__ Mat<D> shfl_down_mat(const Mat<D>& m, int delta) {

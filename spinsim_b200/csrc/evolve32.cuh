@@ -94,23 +94,6 @@ SS_D Su2f su2_prod(const Su2f& b, const Su2f& a) {
 
 SS_D Su2f su2_add(const Su2f& a, const Su2f& b) { return Su2f{a.am1 + b.am1, a.beta + b.beta}; }
 
-// Spin-one representation of an FP64 SU(2) element (full matrix, not residual).
-SS_D Mat<3> su2_to_spin_one(const c64& alpha, const c64& beta) {
-    constexpr double r2 = 1.4142135623730951;
-    Mat<3> m;
-    const c64 ac = conj(alpha), bc = conj(beta);
-    m.a[0][0] = alpha * alpha;
-    m.a[1][0] = r2 * (alpha * beta);
-    m.a[2][0] = beta * beta;
-    m.a[0][1] = (-r2) * (alpha * bc);
-    m.a[1][1] = c64{alpha.re * alpha.re + alpha.im * alpha.im - beta.re * beta.re - beta.im * beta.im, 0.0};
-    m.a[2][1] = r2 * (ac * beta);
-    m.a[0][2] = bc * bc;
-    m.a[1][2] = (-r2) * (ac * bc);
-    m.a[2][2] = ac * ac;
-    return m;
-}
-
 // exp(A) - 1 for A = -i H, H = x Jx + y Jy + z Jz + q Q (spin one, Q = diag(1, -2, 1) / 3), by a
 // Taylor series to A^6 / 6! on A scaled to norm <= 1/32 (truncation below 2e-13 relative),
 // followed by residual squarings (E - 1 -> 2 (E - 1) + (E - 1)^2) when it was scaled.

@@ -38,6 +38,11 @@
 // to 1e-11 in the final state.  Instances with more than kBulkTones
 // tones on a channel, or spin one with a quadratic shift, take the per-interval path (interval32,
 // CF4) inside the same kernel.
+//
+// Scan partials.  A CTA tile is one state scan tile (scan.cuh).  Each interval's lab-frame operator is
+// an SU(2) pair (spin one: its representation), so each warp also multiplies its eight rows' pairs
+// with three shuffle rounds and writes the product (4 doubles); the scan's prefix kernel combines a
+// tile's four warp products and the scan launches no tile products pass over U.
 #pragma once
 #include "common.cuh"
 #include "evolve32.cuh"
@@ -93,16 +98,13 @@ SS_D Su2d shfl_down_su2(const Su2d& v, int delta) {
     return o;
 }
 
-SS_D bool dmma_eligible(const FieldDesc& f, int dim) {
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-        if (f.tone_count[c] > kBulkTones) return false;
-    return !(dim == 3 && tones_have_quadratic_shift(f));
-}
+static_assert(kDmmaTile == kScanTile, "a CTA tile is one state scan tile (its warps' row products are its partials)");
 
+// partial_out (may be null): the tile's scan partials, where this warp writes the lab-frame SU(2) pair of
+// its rows' product (later rows from the left; rows past the tile's end are the identity).
 template <int D>
 SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc& f, const Tile& tile, DmmaShared& sh,
-                    double* time_out, double* u_out, float* norms_out) {
+                    double* time_out, double* u_out, float* norms_out, double* partial_out) {
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
@@ -334,27 +336,21 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
         nsq += __shfl_down_sync(0xffffffffu, nsq, sft);
         if ((q & (2 * sft - 1)) == 0) acc = su2d_mul(later, acc);
     }
+    // The interval's lab-frame operator as an SU(2) pair: leaving the frame (I:839-852) multiplies by
+    // the SU(2) element diag(exp(-i phi), exp(i phi)), phi = rw dt_out (spin half, rw halved above) or
+    // rw dt_out / 2 (spin one, whose representation doubles the phase).  Rows past the tile's end and
+    // the other lanes of a quad hold the identity.
+    Su2p v = su2p_identity();
     if (active && q == 0) {
-        Mat<D> u;  // lab-frame operator of the interval
-        const c64 alpha = c64{1.0 + acc.am1.re, acc.am1.im};
-        if constexpr (D == 3) {
-            u = su2_to_spin_one(alpha, acc.beta);
-        } else {
-            u.a[0][0] = alpha;
-            u.a[1][0] = acc.beta;
-            u.a[0][1] = c64{-acc.beta.re, acc.beta.im};
-            u.a[1][1] = conj(alpha);
+        v.a = c64{1.0 + acc.am1.re, acc.am1.im};
+        v.b = acc.beta;
+        if (m.rotating) {
+            c64 wh;
+            sincos(rw * dt_out * (D == 2 ? 1.0 : 0.5), &wh.im, &wh.re);
+            v.a = v.a * conj(wh);
+            v.b = v.b * wh;
         }
-        if (m.rotating) {  // leave the rotating frame, I:839-852
-            c64 wo;
-            sincos(rw * dt_out, &wo.im, &wo.re);
-            const c64 woc = conj(wo);
-#pragma unroll
-            for (int k = 0; k < D; k++) {
-                u.a[0][k] = u.a[0][k] * woc;
-                u.a[D - 1][k] = u.a[D - 1][k] * wo;
-            }
-        }
+        const Mat<D> u = su2p_to_mat<D>(v);
         time_out[idx] = t_c;
         if (norms_out != nullptr) norms_out[idx] = nsq;
         double2* dst = reinterpret_cast<double2*>(u_out) + idx * (D * D);
@@ -362,6 +358,18 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
         for (int r = 0; r < D; r++)
 #pragma unroll
             for (int k = 0; k < D; k++) dst[r * D + k] = make_double2(u.a[r][k].re, u.a[r][k].im);
+    }
+    if (partial_out != nullptr) {  // the warp's product of its rows (lanes 4 g), later rows from the left
+#pragma unroll
+        for (int sft = kDmmaSegments; sft < 32; sft <<= 1) {
+            const Su2p later = shfl_down_su2p(v, sft);
+            if ((lane & (2 * sft - 1)) == 0) v = su2p_mul(later, v);
+        }
+        if (lane == 0) {
+            double2* dst = reinterpret_cast<double2*>(partial_out) + 2 * (threadIdx.x >> 5);
+            dst[0] = make_double2(v.a.re, v.a.im);
+            dst[1] = make_double2(v.b.re, v.b.im);
+        }
     }
 }
 
@@ -392,9 +400,14 @@ SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
         double* u_out = a.u + inst.u_offset;
         float* norms_out = a.step_norms != nullptr ? a.step_norms + inst.out_offset : nullptr;
         const int dim = (DIMS == 0) ? inst.dim : DIMS;
-        if (dmma_eligible(f, dim)) {
-            if (DIMS != 3 && dim == 2) tile_dmma<2>(a.m, inst, f, tile, sh, time_out, u_out, norms_out);
-            else if (DIMS != 2) tile_dmma<3>(a.m, inst, f, tile, sh, time_out, u_out, norms_out);
+        if (tones_on_tensor_path(f, dim)) {
+            double* partial_out = nullptr;
+            if (a.tile_partials != nullptr) {
+                const int64_t k = (a.scan_begin != nullptr ? a.scan_begin[tile.instance] : 0) + tile.first / kScanTile;
+                partial_out = a.tile_partials + k * kScanMat;
+            }
+            if (DIMS != 3 && dim == 2) tile_dmma<2>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out);
+            else if (DIMS != 2) tile_dmma<3>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out);
         } else if (threadIdx.x < tile.count) {
             // more tones than the products take, or a quadratic shift: one interval per thread
             if (DIMS != 3 && dim == 2)

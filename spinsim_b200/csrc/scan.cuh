@@ -6,25 +6,27 @@
 // parallel prefix scan of the d x d operators in FP64 over scan tiles of kScanTile consecutive
 // output steps of one instance (one warp each), with no waits between blocks:
 // A tile is taken by an 8-lane group (four tiles per warp); lane j of the group holds the product of
-// the tile's operators 4 j .. 4 j + 3, so a tile costs three shuffle rounds instead of five.
-//   A  scan_products_kernel: each group multiplies its tile's operators into the tile product.
+// the tile's operators 4 j .. 4 j + 3, so a tile costs three shuffle rounds instead of five.  A warp
+// first copies its four tiles' operators into shared memory with coalesced loads (consecutive lanes,
+// consecutive 16-byte words), and the apply kernel stages the states there for a coalesced write-out.
+//   A  scan_products_kernel: each group multiplies its tile's operators into the tile product.  On the
+//      tensor path (evolve_dmma.cuh) the time evolution writes each tile's four warp products as
+//      SU(2) pairs instead, and A is not launched; B then scans SU(2) pairs (partials mode).
 //   B  scan_prefix_kernel: a warp per instance scans the instance's tile products 32 at a time and
 //      stores every tile's exclusive prefix (and, when asked, the instance's whole product).
 //   C  scan_apply_kernel: each group scans its lanes' products (lane j: U[4j+3] ... U[0] of the
 //      tile), applies the exclusive part times the tile's prefix to psi0 and steps through its
 //      four output steps writing state and spin (get_spin, I:899-959), fused.
-// Spin half and spin one instances share the launches; the tile list holds the spin-half tiles, then
-// the spin-one tiles, each run padded to whole warps (count 0), so a warp's tiles share a dimension.
+// The tile list holds the spin-half tiles, then the spin-one tiles, each run padded to whole warps
+// (count 0); the tile kernels are launched once per spin dimension over its run of tiles.
 #pragma once
 #include "common.cuh"
 
 namespace spinsim {
 
-constexpr int kScanTile = 32;        // output steps per scan tile
-constexpr int kScanPerLane = 4;      // consecutive operators multiplied by one lane
+constexpr int kScanPerLane = 4;      // consecutive operators multiplied by one lane (kScanTile steps per tile)
 constexpr int kScanGroup = kScanTile / kScanPerLane;  // lanes per tile (8)
 constexpr int kScanTilesPerWarp = 32 / kScanGroup;    // 4
-constexpr int kScanMat = 18;         // doubles per stored tile operator (3 x 3 complex; spin half uses 8)
 constexpr int kScanBlock = 128;      // threads per CTA of the scan kernels
 
 template <int D>
@@ -97,6 +99,8 @@ struct ScanArgs {
     double* spin;               // [sum N * 3], may be null
     double* total;              // per instance: U[N-1] ... U[0], complex [d][d]; may be null
     int64_t single_n_out;       // output steps of the single instance (implicit tiles)
+    int32_t partials;           // 1: tile_product holds each tile's four warp partials (SU(2) pairs) written by
+                                // the tensor-path time evolution, in place of the tile products
 };
 
 SS_D const Instance& scan_instance(const ScanArgs& a, int32_t i) { return a.instances[i]; }
@@ -125,25 +129,84 @@ struct DescriptorArgs {
 };
 
 #ifdef __CUDACC__
-// Lane j of the tile's group: U[4j + 3] ... U[4j] of the tile (identity past its end).
+// Shared memory of a scan CTA for spin dimension D: per warp, its four tiles' operators; the apply
+// kernel reuses the area for the tiles' states once every lane has read its operators.  Each lane's
+// four operators (its segment) are padded by one 16-byte word, so that the eight lanes of a group,
+// which read their segments in one phase of a 16-byte load, fall on distinct banks (segment strides
+// of 272 and 592 bytes); staged states are padded the same way (144 and 208 bytes).  Spin-one CTAs
+// take two warps, so both sizes stay within the default 48 KB of dynamic shared memory.
 template <int D>
-SS_D Mat<D> lane_operators(const ScanArgs& a, const Instance& inst, const Tile& tile, int j) {
+struct ScanShared {
+    static constexpr int kWarps = D == 2 ? 4 : 2;
+    static constexpr int kThreads = 32 * kWarps;
+    static constexpr int kOpWords = kScanPerLane * D * D;     // 16-byte words of a lane's operators
+    static constexpr int kSeg = 2 * (kOpWords + 1);          // doubles per lane segment, padded
+    static constexpr int kStateWords = kScanPerLane * D;      // 16-byte words of a lane's states
+    static constexpr int kStateSeg = 2 * (kStateWords + 1);  // doubles, padded
+    static constexpr int kTile = kScanGroup * kSeg;          // doubles per tile
+    static constexpr int kPerWarp = kScanTilesPerWarp * kTile;
+    static constexpr size_t kBytes = sizeof(double) * (size_t)kPerWarp * kWarps;
+    static_assert(kScanGroup * kStateSeg <= kTile, "staged states fit in the operators' area");
+    static_assert(kBytes <= 48 * 1024, "scan tile kernels use the default dynamic shared memory limit");
+};
+
+// A warp's four tiles of operators, copied into shared memory with coalesced loads (one warp-wide
+// pass per tile); lanes then read their four consecutive operators from there.
+template <int D>
+SS_D void stage_operators(const ScanArgs& a, int64_t first_tile, int64_t tile_hi, int lane, double* su) {
+    using S = ScanShared<D>;
     constexpr int MD = 2 * D * D;
-    const double* u = a.u + inst.u_offset + (tile.first + kScanPerLane * j) * MD;
+#pragma unroll
+    for (int t = 0; t < kScanTilesPerWarp; t++) {
+        const Tile tile = scan_tile(a, first_tile + t < tile_hi ? first_tile + t : a.n_tiles);
+        if (tile.count <= 0) continue;
+        const Instance& inst = scan_instance(a, tile.instance);
+        const double2* src = reinterpret_cast<const double2*>(a.u + inst.u_offset + tile.first * MD);
+        double2* dst = reinterpret_cast<double2*>(su + t * S::kTile);
+        const int words = tile.count * D * D;
+#pragma unroll
+        for (int r = 0; r < D * D; r++) {  // a full tile is D * D words per lane
+            const int e = lane + 32 * r;
+            if (e < words) dst[e + e / S::kOpWords] = __ldg(src + e);
+        }
+    }
+    __syncwarp();
+}
+
+template <int D>
+SS_D Mat<D> shared_mat(const double* p) {
+    Mat<D> m;
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int i = 0; i < D; i++)
+#pragma unroll
+        for (int j = 0; j < D; j++) {
+            const double2 v = q[i * D + j];
+            m.a[i][j] = c64{v.x, v.y};
+        }
+    return m;
+}
+
+// Lane j of the tile's group: U[4j + 3] ... U[4j] of the tile (identity past its end), from the
+// tile's operators in shared memory (su: the tile's area).
+template <int D>
+SS_D Mat<D> lane_operators(const double* su, const Tile& tile, int j) {
+    constexpr int MD = 2 * D * D;
+    const double* u = su + j * ScanShared<D>::kSeg;
     const int n = min(kScanPerLane, tile.count - kScanPerLane * j);
     Mat<D> p;
-    if (n > 0) p = load_mat<D>(u);
+    if (n > 0) p = shared_mat<D>(u);
     else set_identity(p);
 #pragma unroll
     for (int i = 1; i < kScanPerLane; i++)
-        if (i < n) p = matmul(load_mat<D>(u + i * MD), p);
+        if (i < n) p = matmul(shared_mat<D>(u + i * MD), p);
     return p;
 }
 
 template <int D>
-SS_D void products_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) {
+SS_D void products_group(const ScanArgs& a, const Tile& tile, int64_t k, int j, const double* su) {
     Mat<D> m;
-    if (tile.count > 0) m = lane_operators<D>(a, scan_instance(a, tile.instance), tile, j);
+    if (tile.count > 0) m = lane_operators<D>(su, tile, j);
     else set_identity(m);
 #pragma unroll
     for (int s = 1; s < kScanGroup; s <<= 1) {  // tree over the group's lanes, later ones from the left
@@ -151,12 +214,6 @@ SS_D void products_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) 
         if ((j & (2 * s - 1)) == 0) m = matmul(later, m);
     }
     if (j == 0 && tile.count > 0) store_mat<D>(a.tile_product + k * kScanMat, m);
-}
-
-// The dimension of a warp's tiles (all its tiles share it; the first is never a padding tile).
-SS_D int warp_dim(const ScanArgs& a, int64_t first_tile) {
-    const Tile t = scan_tile(a, first_tile);
-    return t.count > 0 ? scan_instance(a, t.instance).dim : 2;
 }
 
 #ifdef SPINSIM_SCAN_KERNELS  // the launches themselves are defined once, in the C ABI's unit
@@ -167,14 +224,21 @@ __global__ void put_descriptors_kernel(DescriptorArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(kScanBlock) scan_products_kernel(ScanArgs a) {
-    const int64_t w = ((int64_t)blockIdx.x * kScanBlock + threadIdx.x) >> 5;
+extern __shared__ __align__(16) double scan_smem[];
+
+// Tiles [tile_lo, tile_hi) of spin dimension D (the tile list keeps each dimension's tiles together).
+template <int D>
+__global__ void __launch_bounds__(ScanShared<D>::kThreads) scan_products_kernel(ScanArgs a, int64_t tile_lo,
+                                                                               int64_t tile_hi) {
+    const int64_t w0 =
+        tile_lo + (((int64_t)blockIdx.x * ScanShared<D>::kThreads + threadIdx.x) >> 5) * kScanTilesPerWarp;
     const int lane = threadIdx.x & 31;
-    const int64_t k = w * kScanTilesPerWarp + lane / kScanGroup;
-    if (w * kScanTilesPerWarp >= a.n_tiles) return;
-    const Tile tile = scan_tile(a, k);
-    if (warp_dim(a, w * kScanTilesPerWarp) == 2) products_group<2>(a, tile, k, lane % kScanGroup);
-    else products_group<3>(a, tile, k, lane % kScanGroup);
+    if (w0 >= tile_hi) return;
+    double* su = scan_smem + (threadIdx.x >> 5) * ScanShared<D>::kPerWarp;
+    stage_operators<D>(a, w0, tile_hi, lane, su);
+    const int t = lane / kScanGroup;
+    const int64_t k = w0 + t;
+    products_group<D>(a, scan_tile(a, k < tile_hi ? k : a.n_tiles), k, lane % kScanGroup, su + t * ScanShared<D>::kTile);
 }
 
 #endif
@@ -183,13 +247,15 @@ template <int D>
 SS_D void prefix_warp(const ScanArgs& a, int32_t i, int lane) {
     const int32_t b = a.tile_begin != nullptr ? a.tile_begin[i] : 0;
     const int32_t e = a.tile_end != nullptr ? a.tile_end[i] : (int32_t)a.n_tiles;
-    Mat<D> run;
+    Mat<D> run, next;
     set_identity(run);
+    if (b + lane < e) next = load_mat<D>(a.tile_product + (int64_t)(b + lane) * kScanMat);
+    else set_identity(next);
     for (int32_t c0 = b; c0 < e; c0 += 32) {
         const int32_t k = c0 + lane;
-        Mat<D> p;
-        if (k < e) p = load_mat<D>(a.tile_product + (int64_t)k * kScanMat);
-        else set_identity(p);
+        const Mat<D> p = next;
+        if (c0 + 32 + lane < e) next = load_mat<D>(a.tile_product + (int64_t)(c0 + 32 + lane) * kScanMat);  // prefetch
+        else set_identity(next);
         const Mat<D> incl = warp_scan<D>(p, lane);
         Mat<D> excl = shfl_up_mat(incl, 1);
         if (lane == 0) set_identity(excl);
@@ -199,23 +265,69 @@ SS_D void prefix_warp(const ScanArgs& a, int32_t i, int lane) {
     if (a.total != nullptr && lane == 0) store_mat<D>(a.total + (int64_t)i * 2 * D * D, run);
 }
 
+// Tile k's product from its four warp partials (warp 3's rows are the latest).
+SS_D Su2p tile_from_partials(const ScanArgs& a, int64_t k) {
+    const double2* p = reinterpret_cast<const double2*>(a.tile_product + k * kScanMat);
+    Su2p t;
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        const double2 x = __ldg(p + 2 * w), y = __ldg(p + 2 * w + 1);
+        const Su2p v = Su2p{c64{x.x, x.y}, c64{y.x, y.y}};
+        t = w == 0 ? v : su2p_mul(v, t);
+    }
+    return t;
+}
+
+// prefix_warp on SU(2) pairs (tile products from the time evolution's partials); the stored prefixes
+// and total are the d x d operators.
+template <int D>
+SS_D void prefix_warp_su2(const ScanArgs& a, int32_t i, int lane) {
+    const int32_t b = a.tile_begin != nullptr ? a.tile_begin[i] : 0;
+    const int32_t e = a.tile_end != nullptr ? a.tile_end[i] : (int32_t)a.n_tiles;
+    Su2p run = su2p_identity(), next = su2p_identity();
+    if (b + lane < e) next = tile_from_partials(a, b + lane);
+    for (int32_t c0 = b; c0 < e; c0 += 32) {
+        const int32_t k = c0 + lane;
+        Su2p incl = next;
+        next = c0 + 32 + lane < e ? tile_from_partials(a, c0 + 32 + lane) : su2p_identity();  // prefetch
+#pragma unroll
+        for (int s = 1; s < 32; s <<= 1) {  // lane l receives P[l] ... P[0] of the chunk
+            const Su2p earlier = shfl_up_su2p(incl, s);
+            if (lane >= s) incl = su2p_mul(incl, earlier);
+        }
+        Su2p excl = shfl_up_su2p(incl, 1);
+        if (lane == 0) excl = su2p_identity();
+        if (k < e) store_mat<D>(a.tile_prefix + (int64_t)k * kScanMat, su2p_to_mat<D>(su2p_mul(excl, run)));
+        run = su2p_mul(shfl_su2p(incl, 31), run);  // lane 31's inclusive product (a full chunk)
+    }
+    if (a.total != nullptr && lane == 0) store_mat<D>(a.total + (int64_t)i * 2 * D * D, su2p_to_mat<D>(run));
+}
+
 #ifdef SPINSIM_SCAN_KERNELS
 __global__ void __launch_bounds__(kScanBlock) scan_prefix_kernel(ScanArgs a) {
     const int32_t i = (int32_t)(((int64_t)blockIdx.x * kScanBlock + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= a.n_instances) return;
-    if (scan_instance(a, i).dim == 2) prefix_warp<2>(a, i, lane);
-    else prefix_warp<3>(a, i, lane);
+    const bool half = scan_instance(a, i).dim == 2;
+    if (a.partials) {
+        if (half) prefix_warp_su2<2>(a, i, lane);
+        else prefix_warp_su2<3>(a, i, lane);
+    } else {
+        if (half) prefix_warp<2>(a, i, lane);
+        else prefix_warp<3>(a, i, lane);
+    }
 }
 
 #endif
 
+// The group's tile: lane j computes the states of output steps 4j .. 4j + 3 into hist (n of them).
 template <int D>
-SS_D void apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) {
+SS_D int apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j, const double* su,
+                     c64 (&hist)[kScanPerLane][D]) {
     constexpr int MD = 2 * D * D;
     const Instance& inst = scan_instance(a, tile.instance);
     Mat<D> m;
-    if (tile.count > 0) m = lane_operators<D>(a, inst, tile, j);
+    if (tile.count > 0) m = lane_operators<D>(su, tile, j);
     else set_identity(m);
 #pragma unroll
     for (int s = 1; s < kScanGroup; s <<= 1) {  // inclusive scan over the group's lanes
@@ -225,7 +337,7 @@ SS_D void apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) {
     Mat<D> excl = shfl_up_mat(m, 1);
     if (j == 0) set_identity(excl);
     const int first = kScanPerLane * j;
-    if (tile.count <= first) return;
+    if (tile.count <= first) return 0;
     // psi = (exclusive prefix) (tile prefix) psi0 at output step `first`, then the next three steps
     const Mat<D> pre = load_mat<D>(a.tile_prefix + k * kScanMat);
     c64 v[D], psi[D];
@@ -243,25 +355,14 @@ SS_D void apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) {
         for (int c = 1; c < D; c++) acc = cfma(excl.a[r][c], v[c], acc);
         psi[r] = acc;
     }
-    const int64_t i0 = tile.first + first;
-    const double* u = a.u + inst.u_offset + i0 * MD;
-    double2* st = reinterpret_cast<double2*>(a.state + inst.state_offset) + i0 * D;
-    double* sp = a.spin != nullptr ? a.spin + (inst.out_offset + i0) * 3 : nullptr;
+    const double* u = su + j * ScanShared<D>::kSeg;
     const int n = min(kScanPerLane, tile.count - first);
 #pragma unroll
     for (int i = 0; i < kScanPerLane; i++) {
-        if (i >= n) break;
 #pragma unroll
-        for (int r = 0; r < D; r++) st[i * D + r] = make_double2(psi[r].re, psi[r].im);
-        if (sp != nullptr) {
-            double s3[3];
-            spin_of<D>(psi, s3);
-            sp[3 * i + 0] = s3[0];
-            sp[3 * i + 1] = s3[1];
-            sp[3 * i + 2] = s3[2];
-        }
+        for (int r = 0; r < D; r++) hist[i][r] = psi[r];
         if (i + 1 < n) {
-            const Mat<D> op = load_mat<D>(u + i * MD);
+            const Mat<D> op = shared_mat<D>(u + i * MD);
             c64 nx[D];
 #pragma unroll
             for (int r = 0; r < D; r++) {
@@ -274,17 +375,59 @@ SS_D void apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j) {
             for (int r = 0; r < D; r++) psi[r] = nx[r];
         }
     }
+    return n;
 }
 
 #ifdef SPINSIM_SCAN_KERNELS
-__global__ void __launch_bounds__(kScanBlock) scan_apply_kernel(ScanArgs a) {
-    const int64_t w = ((int64_t)blockIdx.x * kScanBlock + threadIdx.x) >> 5;
+template <int D>
+__global__ void __launch_bounds__(ScanShared<D>::kThreads) scan_apply_kernel(ScanArgs a, int64_t tile_lo,
+                                                                            int64_t tile_hi) {
+    const int64_t w0 =
+        tile_lo + (((int64_t)blockIdx.x * ScanShared<D>::kThreads + threadIdx.x) >> 5) * kScanTilesPerWarp;
     const int lane = threadIdx.x & 31;
-    const int64_t k = w * kScanTilesPerWarp + lane / kScanGroup;
-    if (w * kScanTilesPerWarp >= a.n_tiles) return;
-    const Tile tile = scan_tile(a, k);
-    if (warp_dim(a, w * kScanTilesPerWarp) == 2) apply_group<2>(a, tile, k, lane % kScanGroup);
-    else apply_group<3>(a, tile, k, lane % kScanGroup);
+    if (w0 >= tile_hi) return;
+    using S = ScanShared<D>;
+    double* su = scan_smem + (threadIdx.x >> 5) * S::kPerWarp;
+    stage_operators<D>(a, w0, tile_hi, lane, su);
+    const int t = lane / kScanGroup;
+    const int j = lane % kScanGroup;
+    const int64_t k = w0 + t;
+    c64 hist[kScanPerLane][D];
+    const int n = apply_group<D>(a, scan_tile(a, k < tile_hi ? k : a.n_tiles), k, j, su + t * ScanShared<D>::kTile, hist);
+    __syncwarp();  // every lane is done with the operators: the area now takes the states
+    double2* st = reinterpret_cast<double2*>(su + t * S::kTile + j * S::kStateSeg);
+#pragma unroll
+    for (int i = 0; i < kScanPerLane; i++)
+        if (i < n)
+#pragma unroll
+            for (int r = 0; r < D; r++) st[i * D + r] = make_double2(hist[i][r].re, hist[i][r].im);
+    __syncwarp();
+    // coalesced write-out of the four tiles' states; the spin of step e from its staged state
+#pragma unroll
+    for (int tt = 0; tt < kScanTilesPerWarp; tt++) {
+        const Tile tile = scan_tile(a, w0 + tt < tile_hi ? w0 + tt : a.n_tiles);
+        if (tile.count <= 0) continue;
+        const Instance& inst = scan_instance(a, tile.instance);
+        const double2* from = reinterpret_cast<const double2*>(su + tt * S::kTile);
+        double2* to = reinterpret_cast<double2*>(a.state + inst.state_offset) + tile.first * D;
+#pragma unroll
+        for (int r = 0; r < D; r++) {  // a full tile is D words per lane
+            const int e = lane + 32 * r;
+            if (e < tile.count * D) to[e] = from[e + e / S::kStateWords];
+        }
+        if (a.spin != nullptr && lane < tile.count) {
+            const double2* mine = from + lane * D + lane / kScanPerLane;
+            c64 psi[D];
+#pragma unroll
+            for (int r = 0; r < D; r++) psi[r] = c64{mine[r].x, mine[r].y};
+            double s3[3];
+            spin_of<D>(psi, s3);
+            double* sto = a.spin + (inst.out_offset + tile.first + lane) * 3;
+            sto[0] = s3[0];
+            sto[1] = s3[1];
+            sto[2] = s3[2];
+        }
+    }
 }
 #endif  // SPINSIM_SCAN_KERNELS
 #endif

@@ -285,6 +285,61 @@ def test_tensor_path_step_counts_and_tile_edges(cuda):
         assert np.abs(r.state - r1.state).max() < 1e-6, k
 
 
+def _operator_scan(u, psi0):
+    """The state scan of the given operators through spinsim_state (the tile products kernels)."""
+    import ctypes
+    import torch
+    from spinsim_b200 import _lib
+    lib = _lib.load()
+    n, dim = u.shape[0], u.shape[1]
+    ud = torch.from_numpy(np.ascontiguousarray(u)).cuda()
+    state = torch.empty((n, dim), dtype=torch.complex128, device="cuda")
+    ws_bytes = lib.spinsim_state_workspace_size(dim, n)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device="cuda")
+    p0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+    _lib.check(lib.spinsim_state(dim, ud.data_ptr(), n, p0.ctypes.data_as(ctypes.c_void_p), state.data_ptr(), None,
+                                 ws.data_ptr(), ws_bytes, torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    return state.cpu().numpy()
+
+
+def test_tensor_path_partials_scan_equals_operator_scan(cuda):
+    """On the tensor path the time evolution writes each scan tile's warp partials (SU(2) pairs) and
+    the scan skips its tile products: the states equal the scan of the returned operators through
+    spinsim_state to FP64 rounding, for tiles that end inside a warp's rows, instances of more than
+    one prefix chunk (32 tiles) and both spins, in a batch and in single Simulator calls."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    H, O1 = ss.SpinQuantumNumber.HALF, ss.SpinQuantumNumber.ONE
+    lengths = [1, 5, 8, 9, 31, 32, 33, 100, 1023, 1024, 1025, 2100]
+    insts = []
+    for j, n in enumerate(lengths):
+        s = H if j % 3 else O1
+        p = F.tone_parameters(np.random.default_rng(1300 + j))
+        insts.append(B.Instance(s, 0.0, n * 1e-6, 50e-9, 1e-6, s.plus_x, sweep_parameters=p, field=tone_field(p)))
+    b = B.Batch(insts, precision=ss.Precision.FP32_BULK, variant=0)
+    info = b.launch_info()
+    assert info["variant"] == 0 and info["scan_partials"] == 1
+    b.run()
+    for k, inst in enumerate(insts):
+        r = b.result(k)
+        assert r.state.shape[0] == lengths[k]
+        ref = _operator_scan(r.time_evolution, inst.spin.plus_x)
+        assert np.abs(r.state - ref).max() < 1e-12, k
+    plain = B.Batch(insts[:4], precision=ss.Precision.FP64)
+    assert plain.launch_info()["scan_partials"] == 0
+    plain.run()
+    for k in range(4):
+        r = plain.result(k)
+        assert np.abs(r.state - _operator_scan(r.time_evolution, insts[k].spin.plus_x)).max() < 1e-12, k
+    for j, s in enumerate([H, O1]):
+        p = F.tone_parameters(np.random.default_rng(1400 + j))
+        sim = ss.Simulator(tone_field(p), s, precision=ss.Precision.FP32_BULK)
+        r = sim.evaluate(0.0, 1500e-6, 50e-9, 1e-6, s.plus_x)
+        ref = _operator_scan(r.time_evolution, s.plus_x)
+        assert np.abs(r.state - ref).max() < 1e-12, s
+
+
 def test_ragged_batch_edge_instances(cuda):
     """A batch mixing an empty instance (t1 == t0), a single output step, K = 1 (dt_int = dt_out), a
     non-integer step ratio (dt_int reset as the reference does) and fewer steps than a warp, against
