@@ -320,12 +320,12 @@ __global__ void __launch_bounds__(kScanBlock) scan_prefix_kernel(ScanArgs a) {
 
 #endif
 
-// The group's tile: lane j computes the states of output steps 4j .. 4j + 3 into hist (n of them).
+// The group's tile: lane j computes the states of output steps 4j .. 4j + 3 into hist (n of them),
+// from the tile's staged operators (su), tile prefix (pre_s, d x d) and psi0 (psi0_s).
 template <int D>
-SS_D int apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j, const double* su,
+SS_D int apply_group(const Tile& tile, int j, const double* su, const double* pre_s, const double* psi0_s,
                      c64 (&hist)[kScanPerLane][D]) {
     constexpr int MD = 2 * D * D;
-    const Instance& inst = scan_instance(a, tile.instance);
     Mat<D> m;
     if (tile.count > 0) m = lane_operators<D>(su, tile, j);
     else set_identity(m);
@@ -339,13 +339,13 @@ SS_D int apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j, cons
     const int first = kScanPerLane * j;
     if (tile.count <= first) return 0;
     // psi = (exclusive prefix) (tile prefix) psi0 at output step `first`, then the next three steps
-    const Mat<D> pre = load_mat<D>(a.tile_prefix + k * kScanMat);
+    const Mat<D> pre = shared_mat<D>(pre_s);
     c64 v[D], psi[D];
 #pragma unroll
     for (int r = 0; r < D; r++) {
         c64 acc = c64{0.0, 0.0};
 #pragma unroll
-        for (int c = 0; c < D; c++) acc = cfma(pre.a[r][c], c64{inst.psi0[2 * c], inst.psi0[2 * c + 1]}, acc);
+        for (int c = 0; c < D; c++) acc = cfma(pre.a[r][c], c64{psi0_s[2 * c], psi0_s[2 * c + 1]}, acc);
         v[r] = acc;
     }
 #pragma unroll
@@ -378,24 +378,73 @@ SS_D int apply_group(const ScanArgs& a, const Tile& tile, int64_t k, int j, cons
     return n;
 }
 
-#ifdef SPINSIM_SCAN_KERNELS
+// Asynchronous global -> shared copies (cp.async): the apply kernel's two-deep pipeline.
+SS_D void cp_async16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+SS_D void cp_async8(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+SS_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+SS_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Shared memory of the apply kernel: per warp kStages buffers (spin half: the group being applied and
+// the next group in flight; spin one: one, which keeps ten warps resident per SM for its longer
+// arithmetic), each with four tiles of padded operators (ScanShared layout), the tile prefix and psi0.
+// Two warps per CTA: 36 KB (spin half) and 39 KB (spin one).
 template <int D>
-__global__ void __launch_bounds__(ScanShared<D>::kThreads) scan_apply_kernel(ScanArgs a, int64_t tile_lo,
-                                                                            int64_t tile_hi) {
-    const int64_t w0 =
-        tile_lo + (((int64_t)blockIdx.x * ScanShared<D>::kThreads + threadIdx.x) >> 5) * kScanTilesPerWarp;
-    const int lane = threadIdx.x & 31;
-    if (w0 >= tile_hi) return;
-    using S = ScanShared<D>;
-    double* su = scan_smem + (threadIdx.x >> 5) * S::kPerWarp;
-    stage_operators<D>(a, w0, tile_hi, lane, su);
+struct ApplyShared {
+    static constexpr int kStages = D == 2 ? 2 : 1;
+    static constexpr int kWarps = 2;
+    static constexpr int kThreads = 32 * kWarps;
+    static constexpr int kPrefix = ScanShared<D>::kTile;      // offset of the tile prefix (2 d^2 doubles)
+    static constexpr int kPsi0 = kPrefix + 2 * D * D;         // offset of psi0 (2 d doubles)
+    static constexpr int kTileStride = kPsi0 + 2 * D;         // doubles per staged tile (16-byte multiple)
+    static constexpr int kBuffer = kScanTilesPerWarp * kTileStride;
+    static constexpr size_t kBytes = sizeof(double) * kStages * (size_t)kBuffer * kWarps;
+    static_assert(kTileStride % 2 == 0, "16-byte aligned tiles");
+    static_assert(kBytes <= 48 * 1024, "the apply kernel uses the default dynamic shared memory limit");
+};
+
+// Issue the copies of tiles w0 .. w0 + 3 into buf (operators, tile prefix, psi0), warp-cooperatively.
+template <int D>
+SS_D void apply_issue(const ScanArgs& a, int64_t w0, int64_t tile_hi, int lane, double* buf) {
+    using S = ApplyShared<D>;
+    constexpr int MD = 2 * D * D;
+#pragma unroll
+    for (int t = 0; t < kScanTilesPerWarp; t++) {
+        const int64_t k = w0 + t;
+        const Tile tile = scan_tile(a, k < tile_hi ? k : a.n_tiles);
+        if (tile.count <= 0) continue;
+        const Instance& inst = scan_instance(a, tile.instance);
+        const double2* src = reinterpret_cast<const double2*>(a.u + inst.u_offset + tile.first * MD);
+        double* tb = buf + t * S::kTileStride;
+        const int words = tile.count * D * D;
+#pragma unroll
+        for (int r = 0; r < D * D; r++) {
+            const int e = lane + 32 * r;
+            if (e < words) cp_async16(tb + 2 * (e + e / ScanShared<D>::kOpWords), src + e);
+        }
+        if (lane < D * D) cp_async16(tb + S::kPrefix + 2 * lane, a.tile_prefix + k * kScanMat + 2 * lane);
+        if (lane < 2 * D) cp_async8(tb + S::kPsi0 + lane, inst.psi0 + lane);
+    }
+}
+
+// Apply tiles w0 .. w0 + 3 from buf and write their states (and spins) out, coalesced.
+template <int D>
+SS_D void apply_tiles(const ScanArgs& a, int64_t w0, int64_t tile_hi, int lane, double* buf) {
+    using S = ApplyShared<D>;
     const int t = lane / kScanGroup;
     const int j = lane % kScanGroup;
     const int64_t k = w0 + t;
+    double* tb = buf + t * S::kTileStride;
     c64 hist[kScanPerLane][D];
-    const int n = apply_group<D>(a, scan_tile(a, k < tile_hi ? k : a.n_tiles), k, j, su + t * ScanShared<D>::kTile, hist);
+    const int n = apply_group<D>(scan_tile(a, k < tile_hi ? k : a.n_tiles), j, tb, tb + S::kPrefix, tb + S::kPsi0, hist);
     __syncwarp();  // every lane is done with the operators: the area now takes the states
-    double2* st = reinterpret_cast<double2*>(su + t * S::kTile + j * S::kStateSeg);
+    double2* st = reinterpret_cast<double2*>(tb + j * ScanShared<D>::kStateSeg);
 #pragma unroll
     for (int i = 0; i < kScanPerLane; i++)
         if (i < n)
@@ -408,12 +457,12 @@ __global__ void __launch_bounds__(ScanShared<D>::kThreads) scan_apply_kernel(Sca
         const Tile tile = scan_tile(a, w0 + tt < tile_hi ? w0 + tt : a.n_tiles);
         if (tile.count <= 0) continue;
         const Instance& inst = scan_instance(a, tile.instance);
-        const double2* from = reinterpret_cast<const double2*>(su + tt * S::kTile);
+        const double2* from = reinterpret_cast<const double2*>(buf + tt * S::kTileStride);
         double2* to = reinterpret_cast<double2*>(a.state + inst.state_offset) + tile.first * D;
 #pragma unroll
         for (int r = 0; r < D; r++) {  // a full tile is D words per lane
             const int e = lane + 32 * r;
-            if (e < tile.count * D) to[e] = from[e + e / S::kStateWords];
+            if (e < tile.count * D) to[e] = from[e + e / ScanShared<D>::kStateWords];
         }
         if (a.spin != nullptr && lane < tile.count) {
             const double2* mine = from + lane * D + lane / kScanPerLane;
@@ -428,6 +477,39 @@ __global__ void __launch_bounds__(ScanShared<D>::kThreads) scan_apply_kernel(Sca
             sto[2] = s3[2];
         }
     }
+}
+
+#ifdef SPINSIM_SCAN_KERNELS
+// Tiles [tile_lo, tile_hi) of spin dimension D in groups of four per warp; persistent warps take every
+// stride-th group, with kStages groups' copies in flight (spin half: the next group is copied while the
+// current one is applied).
+template <int D>
+__global__ void __launch_bounds__(ApplyShared<D>::kThreads) scan_apply_kernel(ScanArgs a, int64_t tile_lo,
+                                                                             int64_t tile_hi) {
+    using S = ApplyShared<D>;
+    const int lane = threadIdx.x & 31;
+    const int64_t groups = (tile_hi - tile_lo + kScanTilesPerWarp - 1) / kScanTilesPerWarp;
+    const int64_t stride = (int64_t)gridDim.x * S::kWarps;
+    int64_t g = (int64_t)blockIdx.x * S::kWarps + (threadIdx.x >> 5);
+    if (g >= groups) return;  // warp-uniform
+    double* buf0 = scan_smem + (threadIdx.x >> 5) * S::kStages * S::kBuffer;
+#pragma unroll
+    for (int st = 0; st < S::kStages; st++) {
+        if (g + st * stride < groups)
+            apply_issue<D>(a, tile_lo + kScanTilesPerWarp * (g + st * stride), tile_hi, lane, buf0 + st * S::kBuffer);
+        cp_async_commit();
+    }
+    for (int it = 0; g < groups; it = (it + 1) % S::kStages, g += stride) {
+        double* buf = buf0 + it * S::kBuffer;
+        cp_async_wait<S::kStages - 1>();  // this buffer's copies have landed (later ones may be in flight)
+        __syncwarp();
+        apply_tiles<D>(a, tile_lo + kScanTilesPerWarp * g, tile_hi, lane, buf);
+        __syncwarp();  // the write-out has read the buffer before it is refilled
+        if (g + S::kStages * stride < groups)
+            apply_issue<D>(a, tile_lo + kScanTilesPerWarp * (g + S::kStages * stride), tile_hi, lane, buf);
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
 }
 #endif  // SPINSIM_SCAN_KERNELS
 #endif
