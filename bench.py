@@ -79,10 +79,11 @@ def instances(ss, specs):
 # frame 14, generators 32, two exponentials 10,920 + 14, two 3x3 products 432, time 1.  FP32-bulk
 # (tensor-path tone kernel, Magnus step): field samples 192 as FP64 tensor-core products (two Gauss
 # points x three channels x 16 multiply-adds) + the phasor table's recurrences 9, frame 26, sum and
-# difference of the samples 6, the SU(2) product into the interval's FP64 operator 33; in FP32 the
-# commutator 15 and one SU(2) exponential 27.  Spin one runs as SU(2) (no quadratic shift here).
+# difference of the samples 6, the exponential's linear part and the SU(2) product into the
+# interval's FP64 operator 39; in FP32 the commutator 15 and the exponential's O(|g|^2) remainder 21.
+# Spin one runs as SU(2) (no quadratic shift here).
 FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
-FLOPS_BULK = {2: {"fp64": 266, "fp32": 42}, 3: {"fp64": 266, "fp32": 42}}
+FLOPS_BULK = {2: {"fp64": 272, "fp32": 36}, 3: {"fp64": 272, "fp32": 36}}
 # DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload
 # (max_registers 168, state scan not run), from one capture of
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve -c 1`.
@@ -227,6 +228,65 @@ def cpu_sample(specs, seconds_target=8.0, n_threads=0):
 
 
 # ------------------------------------------------------------------------------------ our arm
+class PerSpinBatches:
+    """The plain FP64 form run as one launch per spin (spin half and spin one, each with its own
+    autotuned register budget and launch shape), on two streams: a mixed-spin FP64 launch carries the
+    register budget and code of the spin-one Lie-Trotter path into the spin-half steps, so splitting by
+    spin is the faster way to run this batch in FP64."""
+
+    def __init__(self, ss, insts, plans, tune):
+        import torch
+        from spinsim_b200.batch import Batch
+        self.index = {2: [k for k, i in enumerate(insts) if i.spin.dimension == 2],
+                      3: [k for k, i in enumerate(insts) if i.spin.dimension == 3]}
+        self.n = len(insts)
+        self.parts, self.config, self.tuning = {}, {}, {}
+        for d, idx in self.index.items():
+            if not idx:
+                continue
+            sub = [insts[k] for k in idx]
+            cfg, timing = tune(sub, use_cache=False, precision=ss.Precision.FP64)
+            self.parts[d] = Batch(sub, precision=ss.Precision.FP64, plan_cache=plans, **cfg)
+            self.config[d], self.tuning[d] = cfg, timing
+        self.total_steps = sum(b.total_steps for b in self.parts.values())
+        self.streams = {d: torch.cuda.Stream() for d in self.parts}
+        self._graph = None
+
+    def run(self, with_state=True):
+        import torch
+        cur = torch.cuda.current_stream()
+        for d, b in self.parts.items():
+            self.streams[d].wait_stream(cur)
+            with torch.cuda.stream(self.streams[d]):
+                b.run(with_state=with_state)
+        for d in self.parts:
+            cur.wait_stream(self.streams[d])
+
+    def capture(self):
+        import torch
+        self.run()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run()
+        self._graph = g
+
+    def replay(self):
+        if self._graph is None:
+            self.capture()
+        self._graph.replay()
+
+    def final_states(self):
+        out = [None] * self.n
+        for d, b in self.parts.items():
+            for k, st in zip(self.index[d], b.final_states()):
+                out[k] = st
+        return out
+
+    def launch_info(self):
+        return {str(d): b.launch_info() for d, b in self.parts.items()}
+
+
 def bench_ours(args, world, rank):
     import torch
     import spinsim_b200 as ss
@@ -238,9 +298,8 @@ def bench_ours(args, world, rank):
     plans = {}
     from spinsim_b200.autotune import tune
     cfg_bulk, tune_bulk = tune(insts, use_cache=False, precision=ss.Precision.FP32_BULK)
-    cfg_plain, tune_plain = tune(insts, use_cache=False, precision=ss.Precision.FP64)
     bulk = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans, **cfg_bulk)
-    plain = Batch(insts, precision=ss.Precision.FP64, plan_cache=plans, **cfg_plain)
+    plain = PerSpinBatches(ss, insts, plans, tune)
     assert bulk.total_steps == total_steps
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > L2 (126 MB)
 
@@ -309,6 +368,15 @@ def bench_ours(args, world, rank):
     fp64_peak = measured_fp64_peak()
     achieved = fp64_flops / evolve_s / 1e12
     fp64_plain_flops, _ = algorithmic_flops(specs, "fp64")
+    # plain FP64 per spin (separate launches): time of each part alone, for the per-spin FP64 rates
+    plain_parts = {}
+    for d, b in plain.parts.items():
+        tp = timed(b, 1, evolve_only=True)
+        part_flops, _ = algorithmic_flops([sp for sp in specs if sp[0] == d], "fp64")
+        plain_parts[f"spin_{'half' if d == 2 else 'one'}"] = {
+            "evolve_kernel_ms": 1e3 * tp[0], "fp64_tflops": part_flops / tp[0] / 1e12,
+            "fp64_frac": part_flops / tp[0] / 1e12 / measured_fp64_peak()["tflops"], "steps": b.total_steps,
+            "config": plain.config[d]}
     value = world * total_steps * args.steps / t_bulk_total
     out = {
         "metric": METRIC,
@@ -329,22 +397,32 @@ def bench_ours(args, world, rank):
                    "instances_per_gpu": len(specs), "integration_steps_per_gpu": total_steps,
                    "l2": "256 MB buffer written between timed steps",
                    "autotuned": {"fp32_bulk": {"chosen": cfg_bulk, "launched": bulk.launch_info()},
-                                 "fp64": {"chosen": cfg_plain, "launched": plain.launch_info()}},
+                                 "fp64": {"chosen": {str(d): c for d, c in plain.config.items()},
+                                          "launched": plain.launch_info()}},
                    "threads_per_block": info["threads_per_block"], "registers": info["registers_per_thread"],
                    "tuning_ms": {"fp32_bulk": {k: 1e3 * v["seconds"] for k, v in tune_bulk.items()},
-                                 "fp64": {k: 1e3 * v["seconds"] for k, v in tune_plain.items()}}},
+                                 "fp64": {str(d): {k: 1e3 * v["seconds"] for k, v in t.items()}
+                                          for d, t in plain.tuning.items()}}},
         "latency_ms": {"p50": 1e3 * float(np.percentile(t_bulk, 50)), "p99": 1e3 * float(np.percentile(t_bulk, 99))},
         "plain_fp64": {"value": world * total_steps * args.steps / t_plain_total, "unit": "steps/s",
                        "ms_per_step": 1e3 * t_plain_total / args.steps,
+                       "launches": "one per spin (two streams), each autotuned",
                        "evolve_kernel_ms": 1e3 * float(np.mean(t_evolve_plain)),
-                       "fp64_tflops": fp64_plain_flops / float(np.mean(t_evolve_plain)) / 1e12},
+                       "fp64_tflops": fp64_plain_flops / float(np.mean(t_evolve_plain)) / 1e12,
+                       "fp64_frac": fp64_plain_flops / float(np.mean(t_evolve_plain)) / 1e12 / measured_fp64_peak()["tflops"],
+                       "per_spin": plain_parts,
+                       "flop_count": "sin, cos, sqrt and division count 1 flop each; a spin-half step's 60 "
+                                     "transcendental calls (48 of them the tone field) keep the FP64 pipe busy far "
+                                     "longer than their flop count"},
         "speedup_vs_fp64": t_plain_total / t_bulk_total,
         "state_err": {"max": float(errs.max()), "p50": float(np.median(errs)), "p99": float(np.percentile(errs, 99)),
                       "tolerance": 1e-6, "vs": "plain FP64 form, final state state[N-1] per instance"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak["tflops"], "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak["tflops"], "traffic": TRAFFIC_BYTES_PER_LAUNCH,
                      "algorithmic_bytes": algorithmic_bytes(specs),
-                     "kernel": "spinsim::evolve_kernel (FP32-bulk, mixed dims, tones)",
+                     "kernel": ("spinsim::evolve_dmma_kernel (FP32-bulk tensor path: field samples as FP64 "
+                                "mma.m8n8k4 products, Magnus step, mixed spins)" if info["variant"] == 0 else
+                                "spinsim::evolve_kernel (FP32-bulk warp tone synthesis, mixed spins)"),
                      "peak_source": fp64_peak["source"],
                      "fp32_achieved": fp32_flops / evolve_s / 1e12,
                      "kernel_ms": 1e3 * evolve_s},
@@ -443,11 +521,11 @@ def bench_serving(args):
     rates = [float(r) for r in args.rates.split(",")]
     out = {"metric": "serving p50/p99 latency and steps/s", "workload": "serving", "requests_per_rate": args.requests,
            "precision": "fp32_bulk", "hbm_budget_gb": args.hbm_budget_gb, "rates": {}}
-    for rate in rates:
-        reqs = synthetic_requests(args.requests, rate, seed=4)
-        kw = {"max_registers": args.max_registers} if args.max_registers > 0 else {}
-        if args.max_steps_per_launch > 0:
-            kw["max_steps_per_launch"] = args.max_steps_per_launch
+    kw = {"max_registers": args.max_registers} if args.max_registers > 0 else {}
+    if args.max_steps_per_launch > 0:
+        kw["max_steps_per_launch"] = args.max_steps_per_launch
+
+    def serve(reqs):
         srv = Server(precision=ss.Precision.FP32_BULK, hbm_budget=int(args.hbm_budget_gb * (1 << 30)),
                      streams=args.streams, max_batch=args.max_batch, **kw)
         torch.cuda.synchronize()
@@ -458,10 +536,35 @@ def bench_serving(args):
         summ.update({"launches": srv.stats["launches"], "budget_waits": srv.stats["budget_waits"],
                      "arena_retries": srv.stats["arena_retries"],
                      "launch_ms_p50": 1e3 * float(np.percentile(dur, 50)), "launch_ms_max": 1e3 * float(max(dur)),
-                     "requests_per_launch_mean": float(np.mean([n for n, _, _, _ in srv.launch_log]))})
+                     "requests_per_launch_mean": float(np.mean([n for n, _, _, _ in srv.launch_log])),
+                     # host time of the serving loop: packing and issuing launches, and completing them
+                     "host_ms": {"admit": 1e3 * srv.stats["host_admit_s"], "complete": 1e3 * srv.stats["host_complete_s"],
+                                 "admit_per_launch": 1e3 * srv.stats["host_admit_s"] / max(1, srv.stats["launches"]),
+                                 "busy_fraction_of_span": (srv.stats["host_admit_s"] + srv.stats["host_complete_s"]) /
+                                                          max(summ["span_s"], 1e-9)}})
+        return summ
+
+    # capacity: the same mix with every request present at the start (the server saturated), and the
+    # device alone: all of these requests as one batched launch, timed with CUDA events
+    cap_reqs = synthetic_requests(args.requests, 1e12, seed=4)
+    capacity = serve(cap_reqs)
+    steps_per_request = float(np.mean([r.steps() for r in cap_reqs]))
+    from spinsim_b200.batch import Batch
+    one = Batch(cap_reqs, precision=ss.Precision.FP32_BULK, **kw)
+    device_s = _event_time(one.run)
+    out["capacity"] = {"steps_per_s": capacity["steps_per_s"], "requests_per_s": capacity["steps_per_s"] / steps_per_request,
+                       "mean_steps_per_request": steps_per_request, "launches": capacity["launches"],
+                       "host_ms": capacity["host_ms"],
+                       "device_steps_per_s": one.total_steps / device_s,
+                       "how": "all requests arrive at t = 0; steps/s over the span to the last completion "
+                              "(device_steps_per_s: the same requests as one launch with state and spin)"}
+    del one
+    for rate in rates:
+        summ = serve(synthetic_requests(args.requests, rate, seed=4))
+        summ["offered_steps_per_s"] = rate * steps_per_request
+        summ["load"] = rate * steps_per_request / capacity["steps_per_s"]  # above 1: latency grows with the backlog
         out["rates"][str(int(rate))] = summ
         print(json.dumps({"rate": rate, **summ}), file=sys.stderr, flush=True)
-        del srv, done
     return out
 
 
@@ -551,6 +654,8 @@ def profile_case(args):
     specs = workload()
     if args.profile_size == "small":
         specs = [(d, min(t, 1e-3), p) for d, t, p in specs[:256]]
+    if args.profile_spin != "mixed":  # one spin's instances (the plain FP64 form runs one launch per spin)
+        specs = [sp for sp in specs if sp[0] == (2 if args.profile_spin == "half" else 3)]
     prec = ss.Precision.FP32_BULK if args.precision == "fp32_bulk" else ss.Precision.FP64
     b = Batch(instances(ss, specs), precision=prec, max_registers=args.max_registers, lanes=args.lanes,
               variant=args.variant)
@@ -573,6 +678,7 @@ def main():
     ap.add_argument("--line-requests", type=int, default=2000, help="serving requests per rate in the main line")
     ap.add_argument("--workload", default="batch", choices=["batch", "serving", "configs", "profile"])
     ap.add_argument("--profile-size", default="small", choices=["small", "full"])
+    ap.add_argument("--profile-spin", default="mixed", choices=["mixed", "half", "one"])
     ap.add_argument("--precision", default="fp32_bulk", choices=["fp32_bulk", "fp64"])
     ap.add_argument("--max-registers", type=int, default=168)
     ap.add_argument("--lanes", type=int, default=0)

@@ -78,6 +78,7 @@ class TabulatedField(BuiltinField):
         if gain is not None:
             for c, v in (gain.items() if isinstance(gain, dict) else enumerate(gain)):
                 self.gain[_channel_index(c)] = v
+        self._cplan()  # the packing plan of these snapshots, made once here rather than at each launch
 
     def device_struct(self, device):
         import torch

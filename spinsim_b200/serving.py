@@ -436,7 +436,9 @@ class Server:
                 fut.set_exception(e)
 
     def _complete(self, inflight, free_streams, done, clock, t0, on_complete, keep_results):
-        """Resolve the launches whose event has passed; returns the launches still running."""
+        """Resolve the launches whose event has passed; returns the launches still running (host time
+        spent here accumulates in stats["host_complete_s"])."""
+        h0 = time.perf_counter()
         still = []
         for item in inflight:
             b, ev, reqs, si, adm = item
@@ -454,11 +456,20 @@ class Server:
             free_streams.append(si)
             self.stats["launches"] += 1
             self.launch_log.append((len(reqs), b.total_steps, adm, tdone))
+        self.stats["host_complete_s"] += time.perf_counter() - h0
         return still
 
     def _admit(self, queue, inflight, free_streams, clock, t0):
         """Start one launch from the head of the queue on a free stream; False when nothing fits
-        (wait for a completion or a released result)."""
+        (wait for a completion or a released result).  Host time spent here (packing descriptors and
+        issuing the launch) accumulates in stats["host_admit_s"]."""
+        h0 = time.perf_counter()
+        try:
+            return self._admit_one(queue, inflight, free_streams, clock, t0)
+        finally:
+            self.stats["host_admit_s"] += time.perf_counter() - h0
+
+    def _admit_one(self, queue, inflight, free_streams, clock, t0):
         avail = self.arena.largest_free()
         take, nbytes, steps = [], 0, 0
         while queue and len(take) < self.max_batch:
