@@ -84,10 +84,11 @@ def instances(ss, specs):
 # Spin one runs as SU(2) (no quadratic shift here).
 FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
 FLOPS_BULK = {2: {"fp64": 272, "fp32": 36}, 3: {"fp64": 272, "fp32": 36}}
-# DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload
-# (max_registers 168, state scan not run), from one capture of
-# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve -c 1`.
-TRAFFIC_BYTES_PER_LAUNCH = 1834240 + 81415168
+# DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload (the
+# tensor-path kernel at 96 registers, writing the scan's tile partials), from one capture of
+# `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve_dmma -c 1`
+# on `bench.py --workload profile --profile-size full --precision fp32_bulk --max-registers 96 --variant 0`.
+TRAFFIC_BYTES_PER_LAUNCH = 2400256 + 91634432
 
 
 def algorithmic_bytes(specs):
