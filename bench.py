@@ -427,8 +427,9 @@ def bench_ours(args, world, rank):
                      "peak_source": fp64_peak["source"],
                      "fp32_achieved": fp32_flops / evolve_s / 1e12,
                      "kernel_ms": 1e3 * evolve_s},
-        # per timed step: the time-evolution kernel and the scan's products, prefix and apply kernels
-        "gpu_launches": 4 * args.steps,
+        # per timed step (one graph replay): the tensor path's per-instance constants, the time
+        # evolution, the scan's prefix, and one apply launch per spin present
+        "gpu_launches": (int(info["variant"] == 0) + 2 + len({d for d, _, _ in specs})) * args.steps,
         "clocks": clocks.summary(),
         "e2e": {"value": world * total_steps * len(e2e_times) / e2e_total, "unit": "steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

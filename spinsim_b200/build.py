@@ -131,6 +131,13 @@ def gen_sources():
             units.append(("sass", name, src))
             reg_decl.append(f'extern "C" const void* spinsim_kget_{name}(void);')
             dmma_rows.append(f"    {{{dims}, {minb}, spinsim_kget_{name}}},")
+    # the tensor path's per-instance constants (one small launch before the time evolution)
+    src = os.path.join(GEN, "k_dmma_consts.cu")
+    write_if_changed(src, '#define SPINSIM_DMMA_CONSTS_KERNEL 1\n#include "evolve_dmma.cuh"\n'
+                          'extern "C" const void* spinsim_kget_dmma_consts(void) {\n'
+                          '    return (const void*)&spinsim::dmma_consts_kernel;\n}\n')
+    units.append(("sass", "dmma_consts", src))
+    reg_decl.append('extern "C" const void* spinsim_kget_dmma_consts(void);')
     reg = ("// generated by spinsim_b200/build.py\n" + "\n".join(reg_decl) +
            "\nstatic const BuiltinEntry kBuiltin[] = {\n" + "\n".join(builtin_rows) + "\n};\n"
            "static const UserEntry kUser[] = {\n" + "\n".join(user_rows) + "\n};\n"

@@ -106,6 +106,8 @@ struct EvolveArgs {
                              // warp's product of its rows as an SU(2) pair in the lab frame (4 doubles per
                              // warp, warp after warp); null: not written
     const int32_t* scan_begin;  // per instance: its first scan tile (null: one instance, tile 0)
+    const struct DmmaConsts* dmma_consts;  // tensor path: per instance, written by dmma_consts_kernel
+                                           // earlier in the launch (null: each tile computes them)
 };
 
 // State scan tiles (scan.cuh): consecutive output steps of one instance per tile, and the doubles
@@ -117,6 +119,19 @@ constexpr int kScanMat = 18;
 // Shared memory of the FP32-bulk tone kernels (see evolve32.cuh), per warp.
 constexpr int kBulkTones = 8;               // tones per channel (x, y, z) synthesised per warp
 constexpr int kToneSlots = 3 * kBulkTones;  // slot = channel * kBulkTones + tone
+
+// Per-instance constants of the tensor-path kernel (evolve_dmma.cuh), the same for all of an
+// instance's tiles: the phasor table's start values exp(i w tau) of every (channel, tone, time
+// segment, Gauss point), each tone's step rotation exp(i w dt) and half-interval phasor
+// exp(i w dt_out / 2), and the choice of step (1: Magnus).
+constexpr int kDmmaRecurrences = 3 * kBulkTones * 4 * 2;
+struct __align__(16) DmmaConsts {
+    double2 z[kDmmaRecurrences];
+    double2 rot[kToneSlots];
+    double2 half_step[kToneSlots];
+    int32_t magnus;
+    int32_t pad[3];
+};
 
 // A tone field whose samples the tensor-path kernel forms as products: at most kBulkTones tones per
 // channel and, for spin one, no quadratic shift (other fields take that kernel's per-interval path).

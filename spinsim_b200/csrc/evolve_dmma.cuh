@@ -53,22 +53,21 @@ constexpr int kDmmaSegments = 4;                             // lanes (time segm
 #ifndef SPINSIM_DMMA_PHASE
 #define SPINSIM_DMMA_PHASE 4
 #endif
-constexpr int kDmmaPhase = SPINSIM_DMMA_PHASE;               // steps per segment in one table buffer
+constexpr int kDmmaPhase = SPINSIM_DMMA_PHASE;
+               // steps per segment in one table buffer
 // Largest step size bound theta = h (|B|max + w_max) for which a tile takes the Magnus step.  The
 // Magnus and CF4 steps differ by O(theta^5) per step: measured 4.6e-6 at theta = 6.7 (one 1 us step)
 // and 1e-11 over 10^6 steps at theta = 0.07, i.e. about 3e-10 theta^5 per step, so at theta <= 0.1
 // below 4e-15 per step, 4e-9 over 10^6 steps.
 constexpr double kMagnusTheta = 0.1;
 constexpr int kDmmaChunkDoubles = 3 * 4 * 32;                // B operands of one step: [channel][k-step][lane]
-constexpr int kDmmaRecurrences = 3 * kBulkTones * kDmmaSegments * 2;  // (channel, tone, segment, Gauss point)
+static_assert(kDmmaRecurrences == 3 * kBulkTones * kDmmaSegments * 2, "(channel, tone, segment, Gauss point)");
 
 struct __align__(16) DmmaShared {
     double table[2][kDmmaPhase][kDmmaChunkDoubles];
     double2 z[kDmmaRecurrences];  // exp(i w tau) of each recurrence at its next step
     double2 rot[3 * kBulkTones];  // exp(i w dt)
     double2 half_step[3 * kBulkTones];  // exp(i w dt_out / 2)
-    double amp_abs[3 * kBulkTones];     // |gain A| and |w| of every tone (the step's size bound)
-    double freq_abs[3 * kBulkTones];
     int32_t tile;
     int32_t magnus;                     // 1: the tile takes the one-exponential Magnus step
 };
@@ -100,11 +99,79 @@ SS_D Su2d shfl_down_su2(const Su2d& v, int delta) {
 
 static_assert(kDmmaTile == kScanTile, "a CTA tile is one state scan tile (its warps' row products are its partials)");
 
+// Recurrence r = ((channel * kBulkTones + tone) * kDmmaSegments + segment) * 2 + Gauss point of an
+// instance with K fine steps of dt: its start phasor exp(i w tau), tau = (segment start) dt + a_lo or
+// a_hi (the reference's sample offsets, I:644-647), and its tone's step rotation exp(i w dt).
+SS_D void dmma_recurrence(const FieldDesc& f, int K, double dt, int r, double2* z, double2* rot) {
+    const int gauss = r & 1, seg = (r >> 1) & (kDmmaSegments - 1), slot = r >> 3;
+    const int c = slot / kBulkTones, tone = slot % kBulkTones;
+    *z = make_double2(0.0, 0.0);
+    *rot = make_double2(1.0, 0.0);
+    if (tone < f.tone_count[c]) {
+        const double a = 0.5 * dt * (gauss ? 1.0 + 1.0 / kSqrt3 : 1.0 - 1.0 / kSqrt3);
+        const double w = __ldg(f.tones + 3 * (f.tone_start[c] + tone));
+        const int start = (int)(((int64_t)K * seg) / kDmmaSegments);
+        double sn, cs;
+        sincos(w * fma((double)start, dt, a), &sn, &cs);
+        *z = make_double2(cs, sn);
+        sincos(w * dt, &sn, &cs);
+        *rot = make_double2(cs, sn);
+    }
+}
+
+// exp(i w dt_out / 2) of tone slot (1 for an absent tone).
+SS_D double2 dmma_half_step(const FieldDesc& f, int slot, double dt_out) {
+    const int c = slot / kBulkTones, tone = slot % kBulkTones;
+    if (tone >= f.tone_count[c]) return make_double2(1.0, 0.0);
+    double sn, cs;
+    sincos(0.5 * __ldg(f.tones + 3 * (f.tone_start[c] + tone)) * dt_out, &sn, &cs);
+    return make_double2(cs, sn);
+}
+
+// 1 when the instance takes the Magnus step: theta = dt (|B|max + w_max) <= kMagnusTheta, |B|max from
+// the channels' biases and amplitudes summed in a fixed order (every launch takes the same branch).
+SS_D int32_t dmma_magnus(const FieldDesc& f, double dt) {
+    double bsq = 0.0, wmax = 0.0;
+    for (int c = 0; c < 3; c++) {
+        double bc = fabs(f.bias[c]);
+        for (int k = 0; k < f.tone_count[c] && k < kBulkTones; k++) {
+            const double* tn = f.tones + 3 * (f.tone_start[c] + k);
+            bc += fabs(f.gain[c] * __ldg(tn + 1));
+            wmax = fmax(wmax, fabs(__ldg(tn)));
+        }
+        bsq = fma(bc, bc, bsq);
+    }
+    return dt * (sqrt(bsq) + wmax) <= kMagnusTheta ? 1 : 0;
+}
+
+#ifdef SPINSIM_DMMA_CONSTS_KERNEL
+// The per-instance constants of the tensor path (DmmaConsts), one CTA of kDmmaRecurrences threads
+// per instance, launched before the time evolution so its tiles load them instead of recomputing
+// them (384 FP64 sincos and the step test per tile).
+__global__ void __launch_bounds__(kDmmaRecurrences) dmma_consts_kernel(EvolveArgs a, DmmaConsts* out, int32_t n) {
+    const int32_t i = blockIdx.x;
+    if (i >= n) return;
+    const Instance& inst = a.instances[i];
+    const FieldDesc& f = a.fields[inst.field];
+    if (!tones_on_tensor_path(f, inst.dim)) return;
+    DmmaConsts& c = out[i];
+    const int r = threadIdx.x;
+    double2 z, rot;
+    dmma_recurrence(f, inst.n_fine, inst.dt_int, r, &z, &rot);
+    c.z[r] = z;
+    if ((r & 7) == 0) c.rot[r >> 3] = rot;
+    if (r < kToneSlots) c.half_step[r] = dmma_half_step(f, r, inst.dt_out);
+    if (r == 0) c.magnus = dmma_magnus(f, inst.dt_int);
+}
+#endif
+
+
 // partial_out (may be null): the tile's scan partials, where this warp writes the lab-frame SU(2) pair of
-// its rows' product (later rows from the left; rows past the tile's end are the identity).
+// its rows' product (later rows from the left; rows past the tile's end are the identity).  cst (may be
+// null): the instance's constants from dmma_consts_kernel; without them the tile computes them.
 template <int D>
 SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc& f, const Tile& tile, DmmaShared& sh,
-                    double* time_out, double* u_out, float* norms_out, double* partial_out) {
+                    double* time_out, double* u_out, float* norms_out, double* partial_out, const DmmaConsts* cst) {
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
@@ -121,24 +188,20 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
     const double half_dt = 0.5 * dt;
     const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)(inst.interval0 + idx)));  // I:818, unfused
 
-    // Producer recurrences r = ((channel * kBulkTones + tone) * kDmmaSegments + segment) * 2 + Gauss point,
-    // started at tau = (segment start) dt + a_lo or a_hi (the reference's sample offsets, I:644-647).
-    for (int r = threadIdx.x; r < kDmmaRecurrences; r += kDmmaThreads) {
-        const int gauss = r & 1, seg = (r >> 1) & (kDmmaSegments - 1), slot = r >> 3;
-        const int c = slot / kBulkTones, tone = slot % kBulkTones;
-        double2 z = make_double2(0.0, 0.0);
-        double2 rot = make_double2(1.0, 0.0);
-        if (tone < f.tone_count[c]) {
-            const double w = __ldg(f.tones + 3 * (f.tone_start[c] + tone));
-            const int start = (int)(((int64_t)K * seg) / kDmmaSegments);
-            double sn, cs;
-            sincos(w * fma((double)start, dt, gauss ? a_hi : a_lo), &sn, &cs);
-            z = make_double2(cs, sn);
-            sincos(w * dt, &sn, &cs);
-            rot = make_double2(cs, sn);
+    // Producer recurrences (dmma_recurrence), their rotations and the step choice: the instance's
+    // constants, or computed here.
+    if (cst != nullptr) {
+        for (int r = threadIdx.x; r < kDmmaRecurrences; r += kDmmaThreads) sh.z[r] = cst->z[r];
+        if (threadIdx.x < kToneSlots) sh.rot[threadIdx.x] = cst->rot[threadIdx.x];
+        if (threadIdx.x == 0) sh.magnus = cst->magnus;
+    } else {
+        for (int r = threadIdx.x; r < kDmmaRecurrences; r += kDmmaThreads) {
+            double2 z, rot;
+            dmma_recurrence(f, K, dt, r, &z, &rot);
+            sh.z[r] = z;
+            if ((r & 7) == 0) sh.rot[r >> 3] = rot;
         }
-        sh.z[r] = z;
-        if ((r & 7) == 0) sh.rot[slot] = rot;
+        if (threadIdx.x == 0) sh.magnus = dmma_magnus(f, dt);
     }
 
     // L of every tone and interval of the tile (buffer 1 of the table holds it until the first refill):
@@ -158,35 +221,18 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
             double sn, cs;
             sincos(fma(w, tq, __ldg(tn + 2)), &sn, &cs);
             l = c64{half_dt * amp * cs, half_dt * amp * sn};
-            sincos(0.5 * w * dt_out, &h.im, &h.re);
+            const double2 hs = cst != nullptr ? cst->half_step[slot] : dmma_half_step(f, slot, dt_out);
+            h = c64{hs.x, hs.y};
             gstep = h * h;
         }
-        if (quarter == 0) {
-            sh.half_step[slot] = make_double2(h.re, h.im);
-            sh.amp_abs[slot] = tone < f.tone_count[c] ? fabs(f.gain[c] * __ldg(f.tones + 3 * (f.tone_start[c] + tone) + 1)) : 0.0;
-            sh.freq_abs[slot] = tone < f.tone_count[c] ? fabs(__ldg(f.tones + 3 * (f.tone_start[c] + tone))) : 0.0;
-        }
+        if (quarter == 0) sh.half_step[slot] = make_double2(h.re, h.im);
 #pragma unroll
         for (int r = 0; r < kDmmaRows; r++) {
             lval[slot * kDmmaTile + kDmmaRows * quarter + r] = make_double2(l.re, l.im);
             l = l * gstep;
         }
     }
-    __syncthreads();  // producer phasors, rotations and L in place
-    if (threadIdx.x == 0) {
-        // Step size bound theta = h (|B|max + w_max), |B|max from the channels' biases and amplitudes
-        // summed in a fixed order (so every launch takes the same branch for the instance).
-        double bsq = 0.0, wmax = 0.0;
-        for (int c = 0; c < 3; c++) {
-            double bc = fabs(f.bias[c]);
-            for (int k = 0; k < kBulkTones; k++) {
-                bc += sh.amp_abs[c * kBulkTones + k];
-                wmax = fmax(wmax, sh.freq_abs[c * kBulkTones + k]);
-            }
-            bsq = fma(bc, bc, bsq);
-        }
-        sh.magnus = dt * (sqrt(bsq) + wmax) <= kMagnusTheta ? 1 : 0;
-    }
+    __syncthreads();  // producer phasors, rotations, step choice and L in place
 
     // A operands: L of this lane's interval for tone 2 s + q / 2 (Re L for even q, Im L for odd q)
     double afr[3][4];
@@ -259,7 +305,8 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
         const int m0 = ph * kDmmaPhase;
         const int mc = min(kDmmaPhase, n_steps - m0);
         const double* tb = &sh.table[ph & 1][0][lane];
-        // The samples of step mm + 1 (tensor path) are formed while step mm's exponentials run.
+        // The samples of step mm + 1 (tensor path) are issued at the end of step mm, so they are in flight
+        // while the next step begins.
         double na[3], nb[3];
         auto samples = [&](int mm, double* xa, double* xb) {
 #pragma unroll
@@ -279,7 +326,6 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
                 sa[c] = na[c];
                 sb[c] = nb[c];
             }
-            if (mm + 1 < mc) samples(mm + 1, na, nb);
             if (active && m0 + mm < seg_len) {
                 if (m.rotating) {  // xy times exp(-i P rw tau), z minus P rw (I:582-618), in units of h / 2
                     const c64 xa = c64{sa[0], sa[1]} * wa;
@@ -313,8 +359,8 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
                     rest.am1.im = fmaf(-0.5f, cz, rest.am1.im);  // the commutator's linear part
                     rest.beta.re = fmaf(0.5f, cy, rest.beta.re);
                     rest.beta.im = fmaf(-0.5f, cx, rest.beta.im);
-                    su2_apply_split(acc, gl64[0], gl64[1], gl64[2], rest);
                     nsq = fmaf(gl[0], gl[0], fmaf(gl[1], gl[1], fmaf(gl[2], gl[2], nsq)));
+                    su2_apply_split(acc, gl64[0], gl64[1], gl64[2], rest);
                 } else {  // the reference's CF4 (I:655-686): two exponentials
                     double ga[3], gb[3];
 #pragma unroll
@@ -325,6 +371,9 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
                     su2_cf4_step(acc, ga, gb, &nsq);
                 }
             }
+            // the next step's samples, issued after this step's arithmetic (all lanes: mma.sync is
+            // warp-collective); measured 0.7% faster than issuing them before it
+            if (mm + 1 < mc) samples(mm + 1, na, nb);
         }
         __syncthreads();  // buffer (ph & 1) is refilled in phase ph + 1
     }
@@ -406,8 +455,9 @@ SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
                 const int64_t k = (a.scan_begin != nullptr ? a.scan_begin[tile.instance] : 0) + tile.first / kScanTile;
                 partial_out = a.tile_partials + k * kScanMat;
             }
-            if (DIMS != 3 && dim == 2) tile_dmma<2>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out);
-            else if (DIMS != 2) tile_dmma<3>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out);
+            const DmmaConsts* cst = a.dmma_consts != nullptr ? a.dmma_consts + tile.instance : nullptr;
+            if (DIMS != 3 && dim == 2) tile_dmma<2>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out, cst);
+            else if (DIMS != 2) tile_dmma<3>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out, cst);
         } else if (threadIdx.x < tile.count) {
             // more tones than the products take, or a quadratic shift: one interval per thread
             if (DIMS != 3 && dim == 2)
