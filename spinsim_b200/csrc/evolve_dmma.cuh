@@ -166,13 +166,27 @@ __global__ void __launch_bounds__(kDmmaRecurrences) dmma_consts_kernel(EvolveArg
 #endif
 
 
+// The interval's lab-frame operator from its SU(2) pair: itself (spin half) or its representation.
+template <int D>
+SS_D void store_interval_operator(const Su2p& v, double* u_out, int64_t idx) {
+    const Mat<D> u = su2p_to_mat<D>(v);
+    double2* dst = reinterpret_cast<double2*>(u_out) + idx * (D * D);
+#pragma unroll
+    for (int r = 0; r < D; r++)
+#pragma unroll
+        for (int k = 0; k < D; k++) dst[r * D + k] = make_double2(u.a[r][k].re, u.a[r][k].im);
+}
+
 // partial_out (may be null): the tile's scan partials, where this warp writes the lab-frame SU(2) pair of
 // its rows' product (later rows from the left; rows past the tile's end are the identity).  cst (may be
-// null): the instance's constants from dmma_consts_kernel; without them the tile computes them.
-template <int D>
+// null): the instance's constants from dmma_consts_kernel; without them the tile computes them.  The
+// spin dimension enters only the frame winding and the stored operator, so a mixed-spin launch
+// (DIMS 0) runs one copy of the step loop for both spins.
+template <int DIMS>
 SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc& f, const Tile& tile, DmmaShared& sh,
                     double* time_out, double* u_out, float* norms_out, double* partial_out, const DmmaConsts* cst) {
-    constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
+    const int D = DIMS != 0 ? DIMS : inst.dim;
+    const int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const int row = (threadIdx.x >> 5) * kDmmaRows + g;
@@ -399,14 +413,10 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
             v.a = v.a * conj(wh);
             v.b = v.b * wh;
         }
-        const Mat<D> u = su2p_to_mat<D>(v);
         time_out[idx] = t_c;
         if (norms_out != nullptr) norms_out[idx] = nsq;
-        double2* dst = reinterpret_cast<double2*>(u_out) + idx * (D * D);
-#pragma unroll
-        for (int r = 0; r < D; r++)
-#pragma unroll
-            for (int k = 0; k < D; k++) dst[r * D + k] = make_double2(u.a[r][k].re, u.a[r][k].im);
+        if (D == 2) store_interval_operator<2>(v, u_out, idx);
+        else store_interval_operator<3>(v, u_out, idx);
     }
     if (partial_out != nullptr) {  // the warp's product of its rows (lanes 4 g), later rows from the left
 #pragma unroll
@@ -420,6 +430,18 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
             dst[1] = make_double2(v.b.re, v.b.im);
         }
     }
+}
+
+// More tones than the products take, or a quadratic shift: one interval per thread (not inlined, so its
+// registers do not weigh on the tensor path's step loop).
+template <int DIMS>
+__device__ __noinline__ void dmma_tile_fallback(const MethodConfig& m, const Instance& inst, const FieldDesc& f,
+                                                int64_t interval, int dim, double* time_out, double* u_out,
+                                                float* norms_out) {
+    if (DIMS != 3 && dim == 2)
+        interval32<2, INTEG_CF4, EXPO_ANALYTIC, FIELD_TONES>(m, inst, f, interval, true, 0, time_out, u_out, norms_out);
+    else if (DIMS != 2)
+        interval32<3, INTEG_CF4, EXPO_LIE_TROTTER, FIELD_TONES>(m, inst, f, interval, true, 0, time_out, u_out, norms_out);
 }
 
 // Persistent launch: CTAs pull tiles of kDmmaTile intervals from the queue (or, without a queue, CTA
@@ -456,16 +478,9 @@ SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
                 partial_out = a.tile_partials + k * kScanMat;
             }
             const DmmaConsts* cst = a.dmma_consts != nullptr ? a.dmma_consts + tile.instance : nullptr;
-            if (DIMS != 3 && dim == 2) tile_dmma<2>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out, cst);
-            else if (DIMS != 2) tile_dmma<3>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out, cst);
+            tile_dmma<DIMS>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out, cst);
         } else if (threadIdx.x < tile.count) {
-            // more tones than the products take, or a quadratic shift: one interval per thread
-            if (DIMS != 3 && dim == 2)
-                interval32<2, INTEG_CF4, EXPO_ANALYTIC, FIELD_TONES>(a.m, inst, f, tile.first + threadIdx.x, true, 0,
-                                                                     time_out, u_out, norms_out);
-            else if (DIMS != 2)
-                interval32<3, INTEG_CF4, EXPO_LIE_TROTTER, FIELD_TONES>(a.m, inst, f, tile.first + threadIdx.x, true, 0,
-                                                                        time_out, u_out, norms_out);
+            dmma_tile_fallback<DIMS>(a.m, inst, f, tile.first + threadIdx.x, dim, time_out, u_out, norms_out);
         }
         __syncthreads();  // shared memory and the tile slot are reused by the next tile
         if (a.tile_counter == nullptr) return;
