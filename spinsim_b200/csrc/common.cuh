@@ -286,6 +286,34 @@ SS_D Mat<D> su2p_to_mat(const Su2p& v) {
     }
 }
 
+// sin x and cos x: for |x| <= 1/2 by their Taylor series (terms to x^15 and x^16, coefficients 1/n!;
+// the first omitted terms are below 2e-17 there, and the results agree with sin and cos to one
+// rounding), else by sincos.  For the small per-interval frame phases of the tensor path.
+SS_D void sincos_small(double x, double* s, double* c) {
+    if (fabs(x) <= 0.5) {
+        const double y = x * x;
+        double q = -1.0 / 1307674368000.0;        // -1/15!
+        q = fma(q, y, 1.0 / 6227020800.0);        //  1/13!
+        q = fma(q, y, -1.0 / 39916800.0);         // -1/11!
+        q = fma(q, y, 1.0 / 362880.0);            //  1/9!
+        q = fma(q, y, -1.0 / 5040.0);             // -1/7!
+        q = fma(q, y, 1.0 / 120.0);               //  1/5!
+        q = fma(q, y, -1.0 / 6.0);                // -1/3!
+        *s = fma(x * y, q, x);
+        double r = 1.0 / 20922789888000.0;        //  1/16!
+        r = fma(r, y, -1.0 / 87178291200.0);      // -1/14!
+        r = fma(r, y, 1.0 / 479001600.0);         //  1/12!
+        r = fma(r, y, -1.0 / 3628800.0);          // -1/10!
+        r = fma(r, y, 1.0 / 40320.0);             //  1/8!
+        r = fma(r, y, -1.0 / 720.0);              // -1/6!
+        r = fma(r, y, 1.0 / 24.0);                //  1/4!
+        r = fma(r, y, -0.5);
+        *c = fma(y, r, 1.0);
+    } else {
+        sincos(x, s, c);
+    }
+}
+
 #ifdef __CUDACC__
 SS_D Su2p shfl_down_su2p(const Su2p& v, int delta) {
     Su2p o;

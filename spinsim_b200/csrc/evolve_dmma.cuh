@@ -282,9 +282,9 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
     // Frame phasors at the Gauss points of this segment's steps: exp(-i P rw (tau - 0)), tau as above
     c64 wa = c64{1.0, 0.0}, wb = c64{1.0, 0.0}, wrot = c64{1.0, 0.0};
     if (m.rotating) {
-        sincos(-prw * dt, &wrot.im, &wrot.re);
-        sincos(-prw * fma((double)seg_start, dt, a_lo), &wa.im, &wa.re);
-        sincos(-prw * fma((double)seg_start, dt, a_hi), &wb.im, &wb.re);
+        sincos_small(-prw * dt, &wrot.im, &wrot.re);
+        sincos_small(-prw * fma((double)seg_start, dt, a_lo), &wa.im, &wa.re);
+        sincos_small(-prw * fma((double)seg_start, dt, a_hi), &wb.im, &wb.re);
     }
 
     // Fill table buffer (ph & 1) with the B operands of steps [ph kDmmaPhase, ...) of every segment.
@@ -409,7 +409,7 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
         v.b = acc.beta;
         if (m.rotating) {
             c64 wh;
-            sincos(rw * dt_out * (D == 2 ? 1.0 : 0.5), &wh.im, &wh.re);
+            sincos_small(rw * dt_out * (D == 2 ? 1.0 : 0.5), &wh.im, &wh.re);
             v.a = v.a * conj(wh);
             v.b = v.b * wh;
         }
