@@ -265,17 +265,28 @@ SS_D void prefix_warp(const ScanArgs& a, int32_t i, int lane) {
     if (a.total != nullptr && lane == 0) store_mat<D>(a.total + (int64_t)i * 2 * D * D, run);
 }
 
-// Tile k's product from its four warp partials (warp 3's rows are the latest).
-SS_D Su2p tile_from_partials(const ScanArgs& a, int64_t k) {
+// A tile's four warp partials (SU(2) pairs), loaded as they are stored; identity past the instance.
+struct TilePartials {
+    double2 v[8];
+};
+
+SS_D TilePartials load_partials(const ScanArgs& a, int64_t k, bool valid) {
+    TilePartials t;
     const double2* p = reinterpret_cast<const double2*>(a.tile_product + k * kScanMat);
-    Su2p t;
+#pragma unroll
+    for (int e = 0; e < 8; e++) t.v[e] = valid ? __ldg(p + e) : make_double2((e & 1) ? 0.0 : 1.0, 0.0);
+    return t;
+}
+
+// The tile's product from its partials (warp 3's rows are the latest).
+SS_D Su2p tile_product_of(const TilePartials& t) {
+    Su2p r;
 #pragma unroll
     for (int w = 0; w < 4; w++) {
-        const double2 x = __ldg(p + 2 * w), y = __ldg(p + 2 * w + 1);
-        const Su2p v = Su2p{c64{x.x, x.y}, c64{y.x, y.y}};
-        t = w == 0 ? v : su2p_mul(v, t);
+        const Su2p v = Su2p{c64{t.v[2 * w].x, t.v[2 * w].y}, c64{t.v[2 * w + 1].x, t.v[2 * w + 1].y}};
+        r = w == 0 ? v : su2p_mul(v, r);
     }
-    return t;
+    return r;
 }
 
 // prefix_warp on SU(2) pairs (tile products from the time evolution's partials); the stored prefixes
@@ -284,12 +295,13 @@ template <int D>
 SS_D void prefix_warp_su2(const ScanArgs& a, int32_t i, int lane) {
     const int32_t b = a.tile_begin != nullptr ? a.tile_begin[i] : 0;
     const int32_t e = a.tile_end != nullptr ? a.tile_end[i] : (int32_t)a.n_tiles;
-    Su2p run = su2p_identity(), next = su2p_identity();
-    if (b + lane < e) next = tile_from_partials(a, b + lane);
+    Su2p run = su2p_identity();
+    TilePartials next = load_partials(a, b + lane, b + lane < e);
     for (int32_t c0 = b; c0 < e; c0 += 32) {
         const int32_t k = c0 + lane;
-        Su2p incl = next;
-        next = c0 + 32 + lane < e ? tile_from_partials(a, c0 + 32 + lane) : su2p_identity();  // prefetch
+        Su2p incl = tile_product_of(next);
+        // the next chunk's partials are loaded here and used in the next iteration (in flight meanwhile)
+        next = load_partials(a, c0 + 32 + lane, c0 + 32 + lane < e);
 #pragma unroll
         for (int s = 1; s < 32; s <<= 1) {  // lane l receives P[l] ... P[0] of the chunk
             const Su2p earlier = shfl_up_su2p(incl, s);
