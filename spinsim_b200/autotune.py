@@ -27,10 +27,10 @@ DEFAULT_CANDIDATES = [
     {"lanes": lanes, "threads_per_block": tpb, "max_registers": regs}
     for regs in (0, 168, 128) for lanes in (1, 2) for tpb in (64, 128)
 ]
-# FP32-bulk tone fields: tensor-path kernel at 102 (spills allowed), 128 and 168 registers; the warp
+# FP32-bulk tone fields: tensor-path kernel at 80 and 96 (6 and 5 CTAs per SM), 128 and 168 registers; the warp
 # synthesis at 168 and 128 registers with 64- or 128-thread CTAs.
 BULK_TONE_CANDIDATES = (
-    [{"variant": 0, "max_registers": regs} for regs in (96, 128, 168)] +
+    [{"variant": 0, "max_registers": regs} for regs in (80, 96, 128, 168)] +
     [{"variant": 1, "max_registers": regs, "threads_per_block": tpb} for regs in (168, 128) for tpb in (64, 128)]
 )
 

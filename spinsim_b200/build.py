@@ -83,7 +83,7 @@ MINB = (2, 3, 4)
 # whose latency-bound table lookups gain from residency more than they lose to spills.
 MINB_TIGHT = (5, 6)
 # Register budgets of the tensor-path tone kernels (128-thread CTAs): 5 -> 102, 4 -> 128, 3 -> 168 registers.
-DMMA_MINB = (3, 4, 5)
+DMMA_MINB = (3, 4, 5, 6)
 
 
 def gen_sources():

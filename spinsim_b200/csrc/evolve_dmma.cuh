@@ -487,7 +487,7 @@ SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
     }
 }
 
-// MINB: minimum resident CTAs per SM for the register allocation (5: 102 registers, 4: 128, 3: 168).
+// MINB: minimum resident CTAs per SM for the register allocation (6: 80 registers, 5: 96, 4: 128, 3: 168).
 template <int DIMS, int MINB>
 __global__ void __launch_bounds__(kDmmaThreads, MINB) evolve_dmma_kernel(EvolveArgs a) {
     __shared__ DmmaShared sh;
