@@ -10,6 +10,7 @@ fixed scan tree), so a result is the same alone and in a mix.
 """
 import ctypes
 from dataclasses import dataclass, field as dc_field
+from operator import attrgetter
 from typing import Any, Optional, Sequence
 
 import numpy as np
@@ -40,6 +41,9 @@ class Instance:
 
 
 INSTANCE_DTYPE = np.dtype(_lib.Instance)
+# what a batch reads of every instance, gathered in one C-level pass
+_INSTANCE_RECORD = attrgetter("spin", "time_start", "time_end", "time_step_integration", "time_step_output",
+                              "state_init", "field")
 
 
 class Batch:
@@ -73,13 +77,18 @@ class Batch:
             raise ValueError("empty batch")
         dev = _cuda_device()
         self.device = dev
-        dims = sorted({i.spin.dimension for i in self.instances})
+        recs = list(map(_INSTANCE_RECORD, self.instances))
+        spins = {id(r[0]): r[0] for r in recs}  # few distinct spin objects
+        dim_of = {k: v.dimension for k, v in spins.items()}
+        dims = sorted(set(dim_of.values()))
         # force_mixed: always the mixed-spin kernel, so results do not depend on the batch's spin mix
         spin_dim = dims[0] if (len(dims) == 1 and not force_mixed) else 0
         if exponentiation_one == ExponentiationMethod.ANALYTIC:
             exponentiation_one = ExponentiationMethod.LIE_TROTTER
         if get_field is None:
-            kinds = {type(i.field).kind if i.field is not None else None for i in self.instances}
+            field_list = [r[6] for r in recs]
+            types = set(map(type, field_list))
+            kinds = {getattr(t, "kind", None) for t in types}
             if len(kinds) != 1 or None in kinds:
                 raise ValueError("without a user get_field every instance needs a built-in field of one kind")
             field_kind = kinds.pop()
@@ -119,13 +128,14 @@ class Batch:
         n = len(self.instances)
         insts = (_lib.Instance * n)()
         rows = {}  # psi0 rows by state_init object (instances often share the basis states)
-        times, psi_rows, dim_list = [], [], []
-        for k, inst in enumerate(self.instances):
-            d = inst.spin.dimension
-            key = (id(inst.state_init), d)
+        dim_list = [dim_of[id(r[0])] for r in recs]
+        psi_rows = []
+        for k, r in enumerate(recs):
+            key = (id(r[5]), dim_list[k])
             row = rows.get(key)
             if row is None:
-                p = np.asarray(inst.state_init, np.complex128).reshape(-1)
+                d = dim_list[k]
+                p = np.asarray(r[5], np.complex128).reshape(-1)
                 if p.size != d:
                     raise ValueError(f"instance {k}: state_init must have {d} entries")
                 row = [0.0] * 6
@@ -133,9 +143,7 @@ class Batch:
                 row[1:2 * d:2] = p.imag.tolist()
                 rows[key] = row
             psi_rows.append(row)
-            dim_list.append(d)
-            times.append((inst.time_start, inst.time_end, inst.time_step_integration, inst.time_step_output))
-        times = np.array(times, np.float64).reshape(n, 4).T.copy()
+        times = np.array([r[1:5] for r in recs], np.float64).reshape(n, 4).T.copy()
         t0, t1, dti, dto = times
         psi0 = np.array(psi_rows, np.float64)
         dims = np.array(dim_list, np.int32)
@@ -155,9 +163,9 @@ class Batch:
         if ws_bytes == 0:
             raise ValueError(_lib.last_error() or "batch layout rejected")
         if get_field is None:
-            from .fields import packed_doubles
-            field_list = [i.field for i in self.instances]
-            field_doubles = max(4, packed_doubles(field_list))
+            from .fields import field_plan
+            plan_rows, packed = field_plan(field_list)
+            field_doubles = max(4, packed)
         else:
             sizes = [max(1, p.size) for p in params_host]
             offs = np.cumsum([0] + sizes[:-1]).astype(np.int64)
@@ -203,8 +211,8 @@ class Batch:
             host_t = torch.from_numpy(np.zeros(field_doubles))
         host = host_t.numpy()
         if get_field is None:
-            from .fields import pack_fields_into
-            fields_arr = pack_fields_into(field_list, host, field_dev.data_ptr())
+            from .fields import pack_plan_into
+            fields_arr = pack_plan_into(plan_rows, n, host, field_dev.data_ptr())
         else:
             from .fields import FIELD_DTYPE
             for p, o in zip(params_host, offs):

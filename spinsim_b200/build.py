@@ -56,12 +56,16 @@ def variants():
     # Mixed-dimension batches: Magnus CF4 with either spin-half exponentiator, spin-one Lie-Trotter.
     out.append((0, 0, 0, 1, 0))
     out.append((0, 0, 1, 1, 0))
-    # FP32-bulk (Magnus CF4): single spin and mixed batches.
+    # FP32-bulk: Magnus CF4 for single spins and mixed batches; Euler and Heun for single spins.
     for eh in (0, 1):
         out.append((2, 0, eh, 1, 1))
     out.append((3, 0, 0, 1, 1))
     out.append((0, 0, 0, 1, 1))
     out.append((0, 0, 1, 1, 1))
+    for integ in (1, 2):
+        for eh in (0, 1):
+            out.append((2, integ, eh, 1, 1))
+        out.append((3, integ, 0, 1, 1))
     return out
 
 

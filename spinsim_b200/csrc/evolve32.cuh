@@ -224,6 +224,27 @@ SS_D void spin_one_cf4_step(Mat<3>& u, const double* ga, const double* gb, float
     apply_split3(u, lin, rest);
 }
 
+// The spin-one Euler step: the 3x3 exponential's linear part in FP64, its remainder in FP32.
+SS_D void spin_one_euler_step(Mat<3>& u, const double* g, float* nsq) {
+    float a[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        a[k] = __double2float_rn(g[k]);
+        *nsq = fmaf(a[k], a[k], *nsq);
+    }
+    const Mat32<3> ra = spin_one_exp_m1(a[0], a[1], a[2], a[3]);
+    c32 la[3][3];
+    spin_one_generator_into<float, c32>(a[0], a[1], a[2], a[3], la);
+    Mat32<3> rest;
+#pragma unroll
+    for (int i2 = 0; i2 < 3; i2++)
+#pragma unroll
+        for (int j2 = 0; j2 < 3; j2++) rest.a[i2][j2] = ra.a[i2][j2] - la[i2][j2];
+    c64 lin[3][3];
+    spin_one_generator_into<double, c64>(g[0], g[1], g[2], g[3], lin);
+    apply_split3(u, lin, rest);
+}
+
 // P <- (1 + E) P in FP64 with E = -i g.sigma/2 (g the step's FP64 generator: the linear part, never
 // rounded to FP32) + rest (its FP32 remainder).
 SS_D void su2_apply_split(Su2d& p, double gx, double gy, double gz, const Su2f& rest) {
@@ -253,13 +274,27 @@ SS_D void su2_cf4_step(Su2d& p, const double* ga, const double* gb, float* nsq) 
     su2_apply_split(p, ga[0] + gb[0], ga[1] + gb[1], ga[2] + gb[2], su2_add(su2_add(ra, rb), prod));
 }
 
+// One Euler step (a single exponential of the generator g, I:759-791) in the same split: the linear
+// part in FP64, the remainder in FP32.
+SS_D void su2_euler_step(Su2d& p, const double* g, float* nsq) {
+    float a[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        a[c] = __double2float_rn(g[c]);
+        *nsq = fmaf(a[c], a[c], *nsq);
+    }
+    su2_apply_split(p, g[0], g[1], g[2], su2_exp_rest(a[0], a[1], a[2]));
+}
+
 // ---------------------------------------------------------------------------------- generic bulk path
-// One output interval per lane (USER and TABLE fields, and tone fields the synthesis below does not
-// take: spin one with a quadratic shift).
+// One output interval per lane (USER and TABLE fields, tone fields the synthesis below does not take:
+// spin one with a quadratic shift, and the Euler and Heun integrators).  The integrators differ only
+// in where a step samples the field and how it weights the samples: Magnus CF4 at the two Gauss
+// points with two exponentials (I:624-686), Heun at the step's ends with two half-step exponentials
+// (I:693-752), Euler at the midpoint with one exponential (I:759-791).
 template <int D, int INTEG, int EXPO, int FIELD>
 SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDesc& f, int64_t index, bool active,
                      int lane_in_group, double* time_out, double* u_out, float* norms_out) {
-    static_assert(INTEG == INTEG_CF4, "the FP32-bulk form is built for Magnus CF4");
     static_assert(EXPO != EXPO_LIE_TROTTER_8, "the FP32-bulk form has no eight-generator exponential");
     constexpr int L = (D == 2) ? 3 : 4;
     constexpr int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
@@ -287,14 +322,19 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     const double a_lo = 0.5 * dt * (1.0 - 1.0 / kSqrt3);
     const double a_hi = 0.5 * dt * (1.0 + 1.0 / kSqrt3);
     const double w0 = (1.5 + kSqrt3) / 6.0, w1 = (1.5 - kSqrt3) / 6.0;
-    const double c0 = dt * w0, c1 = dt * w1;
+    // sample offsets in the step (off_b = dt - off_a) and the weights of the samples in the two
+    // exponentials' generators
+    const double off_a = INTEG == INTEG_CF4 ? a_lo : INTEG == INTEG_HEUN ? 0.0 : 0.5 * dt;
+    const double off_b = INTEG == INTEG_CF4 ? a_hi : dt;
+    const double c0 = INTEG == INTEG_CF4 ? dt * w0 : INTEG == INTEG_HEUN ? 0.5 * dt : dt;
+    const double c1 = INTEG == INTEG_CF4 ? dt * w1 : 0.0;
 
     // Frame phasor W(t) = exp(-i P rw (t - t_c)) by an FP64 recurrence, anchored at this lane's start.
     c64 W = c64{1.0, 0.0}, Wrot = c64{1.0, 0.0}, Woff = c64{1.0, 0.0};
     if (m.rotating && K > 0) {
         sincos(-(double)P * rw * (t_fine - t_c), &W.im, &W.re);
         sincos(-(double)P * rw * dt, &Wrot.im, &Wrot.re);
-        sincos(-(double)P * rw * a_lo, &Woff.im, &Woff.re);
+        sincos(-(double)P * rw * off_a, &Woff.im, &Woff.re);
     }
     TableCursor cur[L];  // per-channel table cursors for the increasing sample times of the steps
 #pragma unroll
@@ -307,24 +347,26 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             s0[k] = 0.0;
             s1[k] = 0.0;
         }
-        sample_field<FIELD, L>(f, t_fine + a_lo, s0, cur);
-        sample_field<FIELD, L>(f, t_fine + a_hi, s1, cur);
+        sample_field<FIELD, L>(f, t_fine + off_a, s0, cur);
+        if (INTEG != INTEG_EULER) sample_field<FIELD, L>(f, t_fine + off_b, s1, cur);
         if (m.rotating) {  // xy times exp(-i P rw tau), z minus P rw
             const c64 Wn = W * Wrot;
             const c64 xa = c64{s0[0], s0[1]} * (W * Woff);
-            const c64 xb = c64{s1[0], s1[1]} * (Wn * conj(Woff));
             s0[0] = xa.re;
             s0[1] = xa.im;
-            s1[0] = xb.re;
-            s1[1] = xb.im;
             s0[2] -= (double)P * rw;
-            s1[2] -= (double)P * rw;
+            if (INTEG != INTEG_EULER) {
+                const c64 xb = c64{s1[0], s1[1]} * (Wn * conj(Woff));
+                s1[0] = xb.re;
+                s1[1] = xb.im;
+                s1[2] -= (double)P * rw;
+            }
             W = Wn;
         }
 #pragma unroll
-        for (int k = 0; k < L; k++) {
+        for (int k = 0; k < L; k++) {  // Euler: the one generator in ga (gb zero)
             ga[k] = fma(c0, s0[k], c1 * s1[k]);
-            gb[k] = fma(c1, s0[k], c0 * s1[k]);
+            gb[k] = INTEG == INTEG_HEUN ? c0 * s1[k] : fma(c1, s0[k], c0 * s1[k]);
         }
     };
 
@@ -347,7 +389,8 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         double na[4] = {0.0, 0.0, 0.0, 0.0}, nb[4] = {0.0, 0.0, 0.0, 0.0};
         t_fine += dt;
         if (j + 1 < j1) step_generators(na, nb);
-        su2_cf4_step(su2, ga, gb, &nsq);
+        if constexpr (INTEG == INTEG_EULER) su2_euler_step(su2, ga, &nsq);
+        else su2_cf4_step(su2, ga, gb, &nsq);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             ga[k] = na[k];
@@ -374,7 +417,8 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             for (; j < j1; j++) {
                 if (!first) step_generators(ga, gb);
                 first = false;
-                spin_one_cf4_step(u, ga, gb, &nsq);
+                if constexpr (INTEG == INTEG_EULER) spin_one_euler_step(u, ga, &nsq);
+                else spin_one_cf4_step(u, ga, gb, &nsq);
                 t_fine += dt;
             }
         }

@@ -16,9 +16,9 @@ namespace spinsim {
 
 template <int DIMS, int INTEG, int EXPO_H, int EXPO_O, int FIELD, int PREC>
 SS_D void evolve_body(const EvolveArgs& a) {
-    // FP32-bulk tone fields are synthesised per warp: every lane takes kSynthIntervals intervals
-    // (the host sets lanes = 1 for these plans).
-    constexpr bool SYNTH = (PREC == PREC_FP32_BULK && FIELD == FIELD_TONES);
+    // FP32-bulk Magnus CF4 tone fields are synthesised per warp: every lane takes kSynthIntervals
+    // intervals (the host sets lanes = 1 for these plans).
+    constexpr bool SYNTH = (PREC == PREC_FP32_BULK && FIELD == FIELD_TONES && INTEG == INTEG_CF4);
     const int lane = threadIdx.x & 31;
     const int lanes = a.m.lanes;
     const int group = lane / lanes;

@@ -212,8 +212,38 @@ TABLE_DTYPE = np.dtype(_lib.Table)
 
 
 def _check_fields(fields):
-    if not all(isinstance(f, (TabulatedField, ToneField)) for f in fields) or len({f.kind for f in fields}) > 1:
+    types = set(map(type, fields))  # one pass at C level; the per-type checks below are few
+    if not all(issubclass(t, (TabulatedField, ToneField)) for t in types) or len({t.kind for t in types}) > 1:
         raise TypeError("packed fields must be built-in fields of one kind")
+
+
+def field_plan(fields):
+    """The packing plan of a list of built-in fields of one kind (``spinsim_pack_fields`` rows) and
+    the float64 entries the packed buffer takes, in one pass over the fields' cached plans."""
+    _check_fields(fields)
+    if not fields:
+        return np.zeros((0, 8), np.int64), 0
+    cps = [f._cplan() for f in fields]
+    plan = np.concatenate([c[0] for c in cps]) if len(cps) > 1 else cps[0][0]
+    doubles = sum([c[1] for c in cps])
+    if fields[0].kind == TabulatedField.kind:  # eight table descriptors per tabulated field
+        doubles += 8 * _TABLE_DOUBLES * len(fields)
+    return plan, doubles
+
+
+def pack_plan_into(plan, n, host, base):
+    """``pack_fields_into`` from a ``field_plan`` of n fields."""
+    out = np.zeros(n, FIELD_DTYPE)
+    if not n:
+        return out
+    if host.dtype != np.float64 or not host.flags["C_CONTIGUOUS"]:
+        raise ValueError("host must be a contiguous float64 array")
+    lib = _lib.load()
+    used = lib.spinsim_pack_fields(n, plan.ctypes.data, plan.shape[0], host.ctypes.data, host.size, int(base),
+                                   out.ctypes.data)
+    if used < 0:
+        _lib.check(int(used))
+    return out
 
 
 def packed_doubles(fields):
@@ -229,20 +259,8 @@ def pack_fields_into(fields, host, base):
     at least ``packed_doubles(fields)`` entries) for a device copy of ``host`` at address ``base``;
     returns the ``spinsim_field`` structs as a numpy array of ``FIELD_DTYPE``.  Layout (the library's
     ``spinsim_pack_fields``): the tabulated fields' descriptors first, then every field's arrays."""
-    _check_fields(fields)
-    n = len(fields)
-    out = np.zeros(n, FIELD_DTYPE)
-    if not n:
-        return out
-    if host.dtype != np.float64 or not host.flags["C_CONTIGUOUS"]:
-        raise ValueError("host must be a contiguous float64 array")
-    plan = np.concatenate([f._cplan()[0] for f in fields]) if n > 1 else fields[0]._cplan()[0]
-    lib = _lib.load()
-    used = lib.spinsim_pack_fields(n, plan.ctypes.data, plan.shape[0], host.ctypes.data, host.size, int(base),
-                                   out.ctypes.data)
-    if used < 0:
-        _lib.check(int(used))
-    return out
+    plan, _ = field_plan(fields)
+    return pack_plan_into(plan, len(fields), host, base)
 
 
 # ---------------------------------------------------------------------------- sampler factory

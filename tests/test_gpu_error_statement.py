@@ -87,3 +87,46 @@ def test_detuned_rabi_sweep_and_simulator(cuda):
     r64 = sim64.evaluate(0, 2e-3, 10e-9, 100e-9, one.plus_z, [deltas[0]])
     assert r64.error_estimate == 0.0
     assert r32.error_estimate >= np.abs(r32.state - r64.state).max()
+
+
+def _tone_field(p):
+    import spinsim_b200 as ss
+    tones = {a: np.array([(p[4 + 24 * a + 3 * k], p[5 + 24 * a + 3 * k], p[6 + 24 * a + 3 * k]) for k in range(8)])
+             for a in range(3)}
+    return ss.ToneField(tones, bias=list(p[:4]))
+
+
+@pytest.mark.parametrize("integration", ["EULER", "HEUN"])
+def test_euler_and_heun_fp32_bulk(cuda, integration):
+    """FP32-bulk with the Euler and Heun integrators (the generic per-interval kernel: one midpoint
+    exponential, or two half-step exponentials at the step's ends, each with its linear part in
+    FP64): within 1e-6 of the FP64 form of the same integrator and within the stated error, on tone
+    batches of both spins (uneven durations) and on user fields through Simulator."""
+    import spinsim_b200 as ss
+    import spinsim_b200.batch as B
+    integ = getattr(ss.IntegrationMethod, integration)
+    half, one = ss.SpinQuantumNumber.HALF, ss.SpinQuantumNumber.ONE
+    plans = {}
+    for spin in (half, one):
+        insts = []
+        for k in range(48):
+            p = F.tone_parameters(np.random.default_rng(2000 + k))
+            dur = float(np.exp(np.random.default_rng(3000 + k).uniform(np.log(5e-6), np.log(300e-6))))
+            insts.append(B.Instance(spin, 0.0, dur, 10e-9, 1e-6, spin.plus_x, sweep_parameters=p, field=_tone_field(p)))
+        kw = dict(integration_method=integ, plan_cache=plans)
+        bulk = B.Batch(insts, precision=ss.Precision.FP32_BULK, **kw)
+        plain = B.Batch(insts, precision=ss.Precision.FP64, **kw)
+        assert bulk.launch_info()["variant"] == -1  # the generic kernel (no tone synthesis for this integrator)
+        bulk.run()
+        plain.run()
+        true = _max_state_error(bulk, plain)
+        assert true.max() < 1e-6, (spin.dimension, true.max())
+        _check(bulk.error_estimates(), true)
+    for spin, field, sweep in ((half, F.gaussian_ensemble, [250.0]), (one, F.detuned_rabi, [1500.0])):
+        sim32 = ss.Simulator(field, spin, integ, precision=ss.Precision.FP32_BULK)
+        sim64 = ss.Simulator(field, spin, integ)
+        r32 = sim32.evaluate(0, 200e-6, 10e-9, 100e-9, spin.plus_z, sweep)
+        r64 = sim64.evaluate(0, 200e-6, 10e-9, 100e-9, spin.plus_z, sweep)
+        err = np.abs(r32.state - r64.state).max()
+        assert err < 1e-6, (spin.dimension, err)
+        assert r32.error_estimate >= err
