@@ -111,7 +111,7 @@ def algorithmic_flops(specs, form):
 
 # ------------------------------------------------------------------------------------ helpers
 class ClockSampler:
-    """SM clock and throttle reasons sampled through NVML every 2 ms during the timed region."""
+    """SM clock and throttle reasons sampled through NVML every 2 ms during the timed regions."""
 
     REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
                "sw_power_cap": 0x4}
@@ -329,10 +329,11 @@ def bench_ours(args, world, rank):
     plain.capture()
     barrier(world)
     torch.cuda.synchronize()
+    # clocks sampled over both timed regions (the FP32-bulk steps, then the plain FP64 steps)
     with ClockSampler(torch.cuda.current_device()) as clocks:
         t_bulk = timed(bulk, args.steps)
+        t_plain = timed(plain, max(1, args.steps // 3))
     t_bulk_total = barrier_max(sum(t_bulk), world)
-    t_plain = timed(plain, max(1, args.steps // 3))
     t_plain_total = barrier_max(sum(t_plain), world) * args.steps / len(t_plain)
 
     # dominant kernel alone (time evolution), same stream, CUDA events
