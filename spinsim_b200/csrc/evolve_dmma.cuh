@@ -51,10 +51,11 @@ namespace spinsim {
 
 constexpr int kDmmaSegments = 4;                             // lanes (time segments) per interval
 #ifndef SPINSIM_DMMA_PHASE
-#define SPINSIM_DMMA_PHASE 4
+#define SPINSIM_DMMA_PHASE 5
 #endif
+// Steps per segment in one table buffer: 5 divides the 25-step segments of K = 100 (1 us output
+// steps of 10 ns), so no phase is a short remainder; 4 was 1% slower there.
 constexpr int kDmmaPhase = SPINSIM_DMMA_PHASE;
-               // steps per segment in one table buffer
 // Largest step size bound theta = h (|B|max + w_max) for which a tile takes the Magnus step.  The
 // Magnus and CF4 steps differ by O(theta^5) per step: measured 4.6e-6 at theta = 6.7 (one 1 us step)
 // and 1e-11 over 10^6 steps at theta = 0.07, i.e. about 3e-10 theta^5 per step, so at theta <= 0.1
