@@ -108,6 +108,8 @@ struct EvolveArgs {
     const int32_t* scan_begin;  // per instance: its first scan tile (null: one instance, tile 0)
     const struct DmmaConsts* dmma_consts;  // tensor path: per instance, written by dmma_consts_kernel
                                            // earlier in the launch (null: each tile computes them)
+    double* rows;  // tensor path: per output step (indexed like time), the interval's lab-frame operator
+                   // as its SU(2) pair (a, b), 4 doubles, for the state scan (null: not written)
 };
 
 // State scan tiles (scan.cuh): consecutive output steps of one instance per tile, and the doubles

@@ -185,7 +185,8 @@ SS_D void store_interval_operator(const Su2p& v, double* u_out, int64_t idx) {
 // (DIMS 0) runs one copy of the step loop for both spins.
 template <int DIMS>
 SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc& f, const Tile& tile, DmmaShared& sh,
-                    double* time_out, double* u_out, float* norms_out, double* partial_out, const DmmaConsts* cst) {
+                    double* time_out, double* u_out, float* norms_out, double* partial_out, const DmmaConsts* cst,
+                    double* rows_out) {
     const int D = DIMS != 0 ? DIMS : inst.dim;
     const int P = (D == 2) ? 2 : 1;  // power of the frame winding in the xy transform (I:599-613)
     const int lane = threadIdx.x & 31;
@@ -418,6 +419,11 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
         if (norms_out != nullptr) norms_out[idx] = nsq;
         if (D == 2) store_interval_operator<2>(v, u_out, idx);
         else store_interval_operator<3>(v, u_out, idx);
+        if (rows_out != nullptr) {  // the same operator as its SU(2) pair, for the state scan
+            double2* r = reinterpret_cast<double2*>(rows_out) + 2 * idx;
+            r[0] = make_double2(v.a.re, v.a.im);
+            r[1] = make_double2(v.b.re, v.b.im);
+        }
     }
     if (partial_out != nullptr) {  // the warp's product of its rows (lanes 4 g), later rows from the left
 #pragma unroll
@@ -479,7 +485,8 @@ SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
                 partial_out = a.tile_partials + k * kScanMat;
             }
             const DmmaConsts* cst = a.dmma_consts != nullptr ? a.dmma_consts + tile.instance : nullptr;
-            tile_dmma<DIMS>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out, cst);
+            double* rows_out = a.rows != nullptr ? a.rows + 4 * inst.out_offset : nullptr;
+            tile_dmma<DIMS>(a.m, inst, f, tile, sh, time_out, u_out, norms_out, partial_out, cst, rows_out);
         } else if (threadIdx.x < tile.count) {
             dmma_tile_fallback<DIMS>(a.m, inst, f, tile.first + threadIdx.x, dim, time_out, u_out, norms_out);
         }

@@ -101,6 +101,8 @@ struct ScanArgs {
     int64_t single_n_out;       // output steps of the single instance (implicit tiles)
     int32_t partials;           // 1: tile_product holds each tile's four warp partials (SU(2) pairs) written by
                                 // the tensor-path time evolution, in place of the tile products
+    const double* rows;         // partials mode: each output step's operator as its SU(2) pair (4 doubles,
+                                // indexed like time), which the apply reads in place of u; may be null
 };
 
 SS_D const Instance& scan_instance(const ScanArgs& a, int32_t i) { return a.instances[i]; }
@@ -390,6 +392,70 @@ SS_D int apply_group(const Tile& tile, int j, const double* su, const double* pr
     return n;
 }
 
+// apply_group on the tile's staged SU(2) pairs (su: lane j's four pairs at j * seg doubles): the lane
+// products and the group's scan are SU(2) products, and each step's d x d operator is formed only
+// to advance the state.
+template <int D>
+SS_D int apply_group_rows(const Tile& tile, int j, const double* su, int seg, const double* pre_s,
+                          const double* psi0_s, c64 (&hist)[kScanPerLane][D]) {
+    const double2* mine = reinterpret_cast<const double2*>(su + j * seg);
+    auto row = [&](int i) {
+        const double2 x = mine[2 * i], y = mine[2 * i + 1];
+        return Su2p{c64{x.x, x.y}, c64{y.x, y.y}};
+    };
+    const int first = kScanPerLane * j;
+    const int n = min(kScanPerLane, tile.count - first);
+    Su2p m = su2p_identity();
+#pragma unroll
+    for (int i = 0; i < kScanPerLane; i++)
+        if (i < n) m = i == 0 ? row(0) : su2p_mul(row(i), m);
+#pragma unroll
+    for (int s = 1; s < kScanGroup; s <<= 1) {  // inclusive scan over the group's lanes
+        const Su2p earlier = shfl_up_su2p(m, s);
+        if (j >= s) m = su2p_mul(m, earlier);
+    }
+    Su2p excl = shfl_up_su2p(m, 1);
+    if (j == 0) excl = su2p_identity();
+    if (tile.count <= first) return 0;
+    // psi = (exclusive prefix) (tile prefix) psi0 at output step `first`, then the next three steps
+    const Mat<D> pre = shared_mat<D>(pre_s);
+    const Mat<D> e = su2p_to_mat<D>(excl);
+    c64 v[D], psi[D];
+#pragma unroll
+    for (int r = 0; r < D; r++) {
+        c64 acc = c64{0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < D; c++) acc = cfma(pre.a[r][c], c64{psi0_s[2 * c], psi0_s[2 * c + 1]}, acc);
+        v[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < D; r++) {
+        c64 acc = e.a[r][0] * v[0];
+#pragma unroll
+        for (int c = 1; c < D; c++) acc = cfma(e.a[r][c], v[c], acc);
+        psi[r] = acc;
+    }
+#pragma unroll
+    for (int i = 0; i < kScanPerLane; i++) {
+#pragma unroll
+        for (int r = 0; r < D; r++) hist[i][r] = psi[r];
+        if (i + 1 < n) {
+            const Mat<D> op = su2p_to_mat<D>(row(i));
+            c64 nx[D];
+#pragma unroll
+            for (int r = 0; r < D; r++) {
+                c64 acc = op.a[r][0] * psi[0];
+#pragma unroll
+                for (int c = 1; c < D; c++) acc = cfma(op.a[r][c], psi[c], acc);
+                nx[r] = acc;
+            }
+#pragma unroll
+            for (int r = 0; r < D; r++) psi[r] = nx[r];
+        }
+    }
+    return n;
+}
+
 // Asynchronous global -> shared copies (cp.async): the apply kernel's two-deep pipeline.
 SS_D void cp_async16(void* dst, const void* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
@@ -403,16 +469,23 @@ SS_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memor
 template <int N>
 SS_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Shared memory of the apply kernel: per warp kStages buffers (spin half: the group being applied and
-// the next group in flight; spin one: one, which keeps ten warps resident per SM for its longer
-// arithmetic), each with four tiles of padded operators (ScanShared layout), the tile prefix and psi0.
-// Two warps per CTA: 36 KB (spin half) and 39 KB (spin one).
-template <int D>
+// Shared memory of the apply kernel: per warp kStages buffers (the group being applied and the next
+// group in flight; spin one from d x d operators: one, which keeps ten warps resident per SM for its
+// longer arithmetic), each with four tiles of staged operators, the tile prefix and psi0.  ROWS: the
+// operators are SU(2) pairs (four per lane segment, padded by one 16-byte word), and the area is as
+// large as the tile's staged states.  Two warps per CTA: 36 KB and 39 KB from d x d operators, 20 KB
+// and 30 KB from SU(2) pairs.
+template <int D, bool ROWS = false>
 struct ApplyShared {
-    static constexpr int kStages = D == 2 ? 2 : 1;
+    static constexpr int kOpWords = ROWS ? 2 * kScanPerLane : ScanShared<D>::kOpWords;  // per lane segment
+    static constexpr int kSeg = 2 * (kOpWords + 1);                                     // doubles, padded
+    static constexpr int kArea = kScanGroup * kSeg > kScanGroup * ScanShared<D>::kStateSeg
+                                     ? kScanGroup * kSeg
+                                     : kScanGroup * ScanShared<D>::kStateSeg;
+    static constexpr int kStages = (D == 2 || ROWS) ? 2 : 1;
     static constexpr int kWarps = 2;
     static constexpr int kThreads = 32 * kWarps;
-    static constexpr int kPrefix = ScanShared<D>::kTile;      // offset of the tile prefix (2 d^2 doubles)
+    static constexpr int kPrefix = kArea;                     // offset of the tile prefix (2 d^2 doubles)
     static constexpr int kPsi0 = kPrefix + 2 * D * D;         // offset of psi0 (2 d doubles)
     static constexpr int kTileStride = kPsi0 + 2 * D;         // doubles per staged tile (16-byte multiple)
     static constexpr int kBuffer = kScanTilesPerWarp * kTileStride;
@@ -421,24 +494,27 @@ struct ApplyShared {
     static_assert(kBytes <= 48 * 1024, "the apply kernel uses the default dynamic shared memory limit");
 };
 
-// Issue the copies of tiles w0 .. w0 + 3 into buf (operators, tile prefix, psi0), warp-cooperatively.
-template <int D>
+// Issue the copies of tiles w0 .. w0 + 3 into buf (operators or SU(2) pairs, tile prefix, psi0),
+// warp-cooperatively.
+template <int D, bool ROWS>
 SS_D void apply_issue(const ScanArgs& a, int64_t w0, int64_t tile_hi, int lane, double* buf) {
-    using S = ApplyShared<D>;
+    using S = ApplyShared<D, ROWS>;
     constexpr int MD = 2 * D * D;
+    constexpr int kWordsPerStep = ROWS ? 2 : D * D;
 #pragma unroll
     for (int t = 0; t < kScanTilesPerWarp; t++) {
         const int64_t k = w0 + t;
         const Tile tile = scan_tile(a, k < tile_hi ? k : a.n_tiles);
         if (tile.count <= 0) continue;
         const Instance& inst = scan_instance(a, tile.instance);
-        const double2* src = reinterpret_cast<const double2*>(a.u + inst.u_offset + tile.first * MD);
+        const double2* src = ROWS ? reinterpret_cast<const double2*>(a.rows + 4 * (inst.out_offset + tile.first))
+                                  : reinterpret_cast<const double2*>(a.u + inst.u_offset + tile.first * MD);
         double* tb = buf + t * S::kTileStride;
-        const int words = tile.count * D * D;
+        const int words = tile.count * kWordsPerStep;
 #pragma unroll
-        for (int r = 0; r < D * D; r++) {
+        for (int r = 0; r < kWordsPerStep; r++) {  // a full tile is kWordsPerStep words per lane
             const int e = lane + 32 * r;
-            if (e < words) cp_async16(tb + 2 * (e + e / ScanShared<D>::kOpWords), src + e);
+            if (e < words) cp_async16(tb + 2 * (e + e / S::kOpWords), src + e);
         }
         if (lane < D * D) cp_async16(tb + S::kPrefix + 2 * lane, a.tile_prefix + k * kScanMat + 2 * lane);
         if (lane < 2 * D) cp_async8(tb + S::kPsi0 + lane, inst.psi0 + lane);
@@ -446,15 +522,18 @@ SS_D void apply_issue(const ScanArgs& a, int64_t w0, int64_t tile_hi, int lane, 
 }
 
 // Apply tiles w0 .. w0 + 3 from buf and write their states (and spins) out, coalesced.
-template <int D>
+template <int D, bool ROWS>
 SS_D void apply_tiles(const ScanArgs& a, int64_t w0, int64_t tile_hi, int lane, double* buf) {
-    using S = ApplyShared<D>;
+    using S = ApplyShared<D, ROWS>;
     const int t = lane / kScanGroup;
     const int j = lane % kScanGroup;
     const int64_t k = w0 + t;
     double* tb = buf + t * S::kTileStride;
     c64 hist[kScanPerLane][D];
-    const int n = apply_group<D>(scan_tile(a, k < tile_hi ? k : a.n_tiles), j, tb, tb + S::kPrefix, tb + S::kPsi0, hist);
+    const Tile tile_k = scan_tile(a, k < tile_hi ? k : a.n_tiles);
+    int n;
+    if constexpr (ROWS) n = apply_group_rows<D>(tile_k, j, tb, S::kSeg, tb + S::kPrefix, tb + S::kPsi0, hist);
+    else n = apply_group<D>(tile_k, j, tb, tb + S::kPrefix, tb + S::kPsi0, hist);
     __syncwarp();  // every lane is done with the operators: the area now takes the states
     double2* st = reinterpret_cast<double2*>(tb + j * ScanShared<D>::kStateSeg);
 #pragma unroll
@@ -495,10 +574,10 @@ SS_D void apply_tiles(const ScanArgs& a, int64_t w0, int64_t tile_hi, int lane, 
 // Tiles [tile_lo, tile_hi) of spin dimension D in groups of four per warp; persistent warps take every
 // stride-th group, with kStages groups' copies in flight (spin half: the next group is copied while the
 // current one is applied).
-template <int D>
-__global__ void __launch_bounds__(ApplyShared<D>::kThreads) scan_apply_kernel(ScanArgs a, int64_t tile_lo,
-                                                                             int64_t tile_hi) {
-    using S = ApplyShared<D>;
+template <int D, bool ROWS>
+__global__ void __launch_bounds__(ApplyShared<D, ROWS>::kThreads) scan_apply_kernel(ScanArgs a, int64_t tile_lo,
+                                                                                   int64_t tile_hi) {
+    using S = ApplyShared<D, ROWS>;
     const int lane = threadIdx.x & 31;
     const int64_t groups = (tile_hi - tile_lo + kScanTilesPerWarp - 1) / kScanTilesPerWarp;
     const int64_t stride = (int64_t)gridDim.x * S::kWarps;
@@ -508,17 +587,17 @@ __global__ void __launch_bounds__(ApplyShared<D>::kThreads) scan_apply_kernel(Sc
 #pragma unroll
     for (int st = 0; st < S::kStages; st++) {
         if (g + st * stride < groups)
-            apply_issue<D>(a, tile_lo + kScanTilesPerWarp * (g + st * stride), tile_hi, lane, buf0 + st * S::kBuffer);
+            apply_issue<D, ROWS>(a, tile_lo + kScanTilesPerWarp * (g + st * stride), tile_hi, lane, buf0 + st * S::kBuffer);
         cp_async_commit();
     }
     for (int it = 0; g < groups; it = (it + 1) % S::kStages, g += stride) {
         double* buf = buf0 + it * S::kBuffer;
         cp_async_wait<S::kStages - 1>();  // this buffer's copies have landed (later ones may be in flight)
         __syncwarp();
-        apply_tiles<D>(a, tile_lo + kScanTilesPerWarp * g, tile_hi, lane, buf);
+        apply_tiles<D, ROWS>(a, tile_lo + kScanTilesPerWarp * g, tile_hi, lane, buf);
         __syncwarp();  // the write-out has read the buffer before it is refilled
         if (g + S::kStages * stride < groups)
-            apply_issue<D>(a, tile_lo + kScanTilesPerWarp * (g + S::kStages * stride), tile_hi, lane, buf);
+            apply_issue<D, ROWS>(a, tile_lo + kScanTilesPerWarp * (g + S::kStages * stride), tile_hi, lane, buf);
         cp_async_commit();
     }
     cp_async_wait<0>();

@@ -84,7 +84,7 @@ class Request:
         (a 120-byte instance and 224-byte field descriptor, time-evolution tiles of 16 bytes per 32
         steps at most, and per scan tile of 32 steps a 16-byte tile and two 144-byte operators: the
         tile's product and prefix, 9.5 bytes per step, counted as 3 d^2; on the tensor path the
-        instance's 3,856-byte kernel constants); the field (tables or tones, 32-byte aligned chunks,
+        instance's 3,856-byte kernel constants and 32 bytes per step of SU(2) pairs); the field (tables or tones, 32-byte aligned chunks,
         and eight 32-byte table descriptors); 256-byte alignment of every piece."""
         d = self.spin.dimension
         n = max(0, int((float(self.time_end) - float(self.time_start)) / float(self.time_step_output)))
@@ -94,7 +94,7 @@ class Request:
             fld += sum(16 * t.size + 48 for t, _, _, _ in tables.values())
         elif self.field is not None and hasattr(self.field, "packed"):
             fld += 8 * self.field.packed()[0].size + 24
-        return n * (33 + 16 * d + 19 * d * d) + 4160 * d * d + 6400 + 4112 + fld
+        return n * (65 + 16 * d + 19 * d * d) + 4160 * d * d + 6400 + 4112 + fld
 
 class Completed:
     """A served request: its ``results`` (made on first access from the launch's arrays), the
