@@ -317,6 +317,13 @@ SS_D void sincos_small(double x, double* s, double* c) {
 }
 
 #ifdef __CUDACC__
+// Programmatic dependent launch (kernels launched with programmatic stream serialization):
+// grid_dependency_wait blocks until the preceding kernel in the stream has completed and its writes
+// are visible; grid_dependency_release lets the following kernel start launching.  Both are no-ops
+// for kernels launched without the attribute.
+SS_D void grid_dependency_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+SS_D void grid_dependency_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 SS_D Su2p shfl_down_su2p(const Su2p& v, int delta) {
     Su2p o;
     o.a.re = __shfl_down_sync(0xffffffffu, v.a.re, delta);

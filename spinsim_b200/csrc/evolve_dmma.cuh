@@ -150,6 +150,7 @@ SS_D int32_t dmma_magnus(const FieldDesc& f, double dt) {
 // per instance, launched before the time evolution so its tiles load them instead of recomputing
 // them (384 FP64 sincos and the step test per tile).
 __global__ void __launch_bounds__(kDmmaRecurrences) dmma_consts_kernel(EvolveArgs a, DmmaConsts* out, int32_t n) {
+    grid_dependency_release();  // the time evolution may start its tiles' set-up meanwhile
     const int32_t i = blockIdx.x;
     if (i >= n) return;
     const Instance& inst = a.instances[i];
@@ -207,6 +208,7 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
     // Producer recurrences (dmma_recurrence), their rotations and the step choice: the instance's
     // constants, or computed here.
     if (cst != nullptr) {
+        grid_dependency_wait();  // the constants' kernel may still be running (it lets this launch start early)
         for (int r = threadIdx.x; r < kDmmaRecurrences; r += kDmmaThreads) sh.z[r] = cst->z[r];
         if (threadIdx.x < kToneSlots) sh.rot[threadIdx.x] = cst->rot[threadIdx.x];
         if (threadIdx.x == 0) sh.magnus = cst->magnus;
@@ -462,7 +464,10 @@ SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
             __syncthreads();
             tile_id = sh.tile;
         }
-        if (tile_id >= a.n_tiles) return;
+        if (tile_id >= a.n_tiles) {
+            grid_dependency_release();  // no tiles left for this CTA: the scan may start launching
+            return;
+        }
         Tile tile;
         if (a.tiles != nullptr) {
             tile = a.tiles[tile_id];

@@ -319,6 +319,7 @@ SS_D void prefix_warp_su2(const ScanArgs& a, int32_t i, int lane) {
 
 #ifdef SPINSIM_SCAN_KERNELS
 __global__ void __launch_bounds__(kScanBlock) scan_prefix_kernel(ScanArgs a) {
+    grid_dependency_wait();  // the tile products (or partials) of the preceding kernel
     const int32_t i = (int32_t)(((int64_t)blockIdx.x * kScanBlock + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (i >= a.n_instances) return;
@@ -573,16 +574,23 @@ SS_D void apply_tiles(const ScanArgs& a, int64_t w0, int64_t tile_hi, int lane, 
 #ifdef SPINSIM_SCAN_KERNELS
 // Tiles [tile_lo, tile_hi) of spin dimension D in groups of four per warp; persistent warps take every
 // stride-th group, with kStages groups' copies in flight (spin half: the next group is copied while the
-// current one is applied).
+// current one is applied).  after_prefix: the preceding kernel is the prefix kernel, whose results
+// this one waits for before it starts; otherwise it follows the other spin's apply kernel, which has
+// already waited for them, so it starts at once and waits for that kernel only before it completes.
 template <int D, bool ROWS>
 __global__ void __launch_bounds__(ApplyShared<D, ROWS>::kThreads) scan_apply_kernel(ScanArgs a, int64_t tile_lo,
-                                                                                   int64_t tile_hi) {
+                                                                                   int64_t tile_hi, int32_t after_prefix) {
     using S = ApplyShared<D, ROWS>;
+    if (after_prefix) grid_dependency_wait();
+    grid_dependency_release();  // the other spin's apply kernel may start: the prefixes are complete
     const int lane = threadIdx.x & 31;
     const int64_t groups = (tile_hi - tile_lo + kScanTilesPerWarp - 1) / kScanTilesPerWarp;
     const int64_t stride = (int64_t)gridDim.x * S::kWarps;
     int64_t g = (int64_t)blockIdx.x * S::kWarps + (threadIdx.x >> 5);
-    if (g >= groups) return;  // warp-uniform
+    if (g >= groups) {  // warp-uniform
+        if (!after_prefix) grid_dependency_wait();
+        return;
+    }
     double* buf0 = scan_smem + (threadIdx.x >> 5) * S::kStages * S::kBuffer;
 #pragma unroll
     for (int st = 0; st < S::kStages; st++) {
@@ -601,6 +609,7 @@ __global__ void __launch_bounds__(ApplyShared<D, ROWS>::kThreads) scan_apply_ker
         cp_async_commit();
     }
     cp_async_wait<0>();
+    if (!after_prefix) grid_dependency_wait();  // complete only after the preceding apply kernel
 }
 #endif  // SPINSIM_SCAN_KERNELS
 #endif
