@@ -458,11 +458,17 @@ __device__ __noinline__ void dmma_tile_fallback(const MethodConfig& m, const Ins
 template <int DIMS>
 SS_D void evolve_dmma_body(const EvolveArgs& a, DmmaShared& sh) {
     int64_t tile_id = blockIdx.x;
+    int32_t reserved = -1;  // thread 0: the next tile, taken from the queue while this one runs
     for (;;) {
         if (a.tile_counter != nullptr) {
-            if (threadIdx.x == 0) sh.tile = atomicAdd(a.tile_counter, 1);
+            if (threadIdx.x == 0) sh.tile = reserved >= 0 ? reserved : atomicAdd(a.tile_counter, 1);
             __syncthreads();
             tile_id = sh.tile;
+            // Away from the end of the queue, take the next tile now (its atomic's latency then passes
+            // during this tile); near the end tiles are taken only when a CTA is free, so no CTA holds
+            // a tile that another could have run.
+            if (threadIdx.x == 0)
+                reserved = tile_id + 2 * (int64_t)gridDim.x < a.n_tiles ? atomicAdd(a.tile_counter, 1) : -1;
         }
         if (tile_id >= a.n_tiles) {
             grid_dependency_release();  // no tiles left for this CTA: the scan may start launching
