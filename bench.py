@@ -85,10 +85,11 @@ def instances(ss, specs):
 FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
 FLOPS_BULK = {2: {"fp64": 272, "fp32": 36}, 3: {"fp64": 272, "fp32": 36}}
 # DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload (the
-# tensor-path kernel at 96 registers, writing the scan's tile partials), from one capture of
+# tensor-path kernel at 96 registers, writing the scan's tile partials and each output step's SU(2)
+# pair beside U: 46 MB of the writes are that scan scratch, not outputs), from one capture of
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve_dmma -c 1`
 # on `bench.py --workload profile --profile-size full --precision fp32_bulk --max-registers 96 --variant 0`.
-TRAFFIC_BYTES_PER_LAUNCH = 2400256 + 91634432
+TRAFFIC_BYTES_PER_LAUNCH = 7344384 + 139672320
 
 
 def algorithmic_bytes(specs):
@@ -298,7 +299,10 @@ def bench_ours(args, world, rank):
     total_steps = sum(int(d / 1e-6) * 100 for _, d, _ in specs)
     plans = {}
     from spinsim_b200.autotune import tune
-    cfg_bulk, tune_bulk = tune(insts, use_cache=False, precision=ss.Precision.FP32_BULK)
+    if args.bulk_config:  # a fixed configuration (profiling runs: the one the untuned run chose)
+        cfg_bulk, tune_bulk = json.loads(args.bulk_config), {}
+    else:
+        cfg_bulk, tune_bulk = tune(insts, use_cache=False, precision=ss.Precision.FP32_BULK)
     bulk = Batch(insts, precision=ss.Precision.FP32_BULK, plan_cache=plans, **cfg_bulk)
     plain = PerSpinBatches(ss, insts, plans, tune)
     assert bulk.total_steps == total_steps
@@ -687,6 +691,9 @@ def main():
     ap.add_argument("--lanes", type=int, default=0)
     ap.add_argument("--variant", type=int, default=0, help="FP32-bulk tone kernel: 0 tensor path, 1 warp synthesis")
     ap.add_argument("--evolve-only", action="store_true")
+    ap.add_argument("--bulk-config", default="",
+                    help='FP32-bulk launch configuration as JSON (e.g. \'{"variant": 0, "max_registers": 96}\') '
+                         "instead of autotuning it; for profiling runs, where serialised kernels distort the tuning")
     ap.add_argument("--e2e-chunks", type=int, default=6, help="groups overlapped in the end-to-end measurement")
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=20000)
