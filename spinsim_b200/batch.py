@@ -10,7 +10,8 @@ fixed scan tree), so a result is the same alone and in a mix.
 """
 import ctypes
 from dataclasses import dataclass, field as dc_field
-from operator import attrgetter
+from itertools import chain
+from operator import attrgetter, itemgetter
 from typing import Any, Optional, Sequence
 
 import numpy as np
@@ -44,6 +45,65 @@ INSTANCE_DTYPE = np.dtype(_lib.Instance)
 # what a batch reads of every instance, gathered in one C-level pass
 _INSTANCE_RECORD = attrgetter("spin", "time_start", "time_end", "time_step_integration", "time_step_output",
                               "state_init", "field")
+_TIMES = itemgetter(1, 2, 3, 4)
+_WORK_RECORD = attrgetter("time_start", "time_end", "time_step_integration", "spin")
+
+
+def _column(records, k):
+    return list(map(itemgetter(k), records))
+
+
+def _dims_of(spins):
+    """int32 array of the spins' dimensions; the per-item work is C-level lookups by object id."""
+    ids = list(map(id, spins))
+    dim_by_id = {k: v.dimension for k, v in dict(zip(ids, spins)).items()}  # few distinct spin objects
+    return np.fromiter(map(dim_by_id.__getitem__, ids), np.int32, len(ids))
+
+
+def _initial_states(states, dims):
+    """(n, 6) float64 rows of interleaved (re, im) initial states, zero padded.  Instances usually
+    share a few basis-state objects, so each distinct object is converted once."""
+    ids = list(map(id, states))
+    distinct = dict(zip(ids, states))
+    slot = {k: j for j, k in enumerate(distinct)}
+    table = np.zeros((len(distinct), 6), np.float64)
+    sizes = np.zeros(len(distinct), np.int32)
+    for j, st in enumerate(distinct.values()):
+        p = np.asarray(st, np.complex128).reshape(-1)
+        sizes[j] = p.size
+        if p.size <= 3:
+            table[j, 0:2 * p.size:2] = p.real
+            table[j, 1:2 * p.size:2] = p.imag
+    idx = np.fromiter(map(slot.__getitem__, ids), np.int64, len(ids))
+    bad = np.flatnonzero(sizes[idx] != dims)
+    if bad.size:
+        k = int(bad[0])
+        raise ValueError(f"instance {k}: state_init must have {int(dims[k])} entries")
+    return table[idx]
+
+
+class _InstanceColumns:
+    """What a batch reads of each instance, in one C-level pass per attribute: the instances, their
+    dimensions (int32), times (n, 4: t0, t1, dt_int, dt_out), initial-state rows (n, 6), fields and
+    piece ranges."""
+
+    __slots__ = ("instances", "dims", "times", "psi0", "fields", "intervals")
+
+    def __init__(self, instances):
+        self.instances = insts = list(instances)
+        n = len(insts)
+        recs = list(map(_INSTANCE_RECORD, insts))
+        self.dims = _dims_of(_column(recs, 0))
+        self.times = np.fromiter(chain.from_iterable(map(_TIMES, recs)), np.float64, 4 * n).reshape(n, 4)
+        self.psi0 = _initial_states(_column(recs, 5), self.dims)
+        self.fields = _column(recs, 6)
+        try:
+            self.intervals = list(map(attrgetter("intervals"), insts))
+        except AttributeError:  # objects with only the other attributes
+            self.intervals = [getattr(i, "intervals", None) for i in insts]
+
+    def __len__(self):
+        return len(self.instances)
 
 
 class Batch:
@@ -72,21 +132,21 @@ class Batch:
                  threads_per_block=0, max_registers=0, plan_cache=None, force_mixed=False, memory=None,
                  staging=None, variant=0):
         import torch
-        self.instances = list(instances)
+        cols = _InstanceColumns(instances)
+        self.instances = cols.instances
         if not self.instances:
             raise ValueError("empty batch")
         dev = _cuda_device()
         self.device = dev
-        recs = list(map(_INSTANCE_RECORD, self.instances))
-        spins = {id(r[0]): r[0] for r in recs}  # few distinct spin objects
-        dim_of = {k: v.dimension for k, v in spins.items()}
-        dims = sorted(set(dim_of.values()))
+        n = len(cols)
+        dims = cols.dims
+        dim_set = sorted(set(dims.tolist()))
         # force_mixed: always the mixed-spin kernel, so results do not depend on the batch's spin mix
-        spin_dim = dims[0] if (len(dims) == 1 and not force_mixed) else 0
+        spin_dim = dim_set[0] if (len(dim_set) == 1 and not force_mixed) else 0
         if exponentiation_one == ExponentiationMethod.ANALYTIC:
             exponentiation_one = ExponentiationMethod.LIE_TROTTER
         if get_field is None:
-            field_list = [r[6] for r in recs]
+            field_list = cols.fields
             types = set(map(type, field_list))
             kinds = {getattr(t, "kind", None) for t in types}
             if len(kinds) != 1 or None in kinds:
@@ -125,34 +185,16 @@ class Batch:
                 plan_cache[key] = plan
 
         # Descriptors and output layout (step normalisation and offsets in the library).
-        n = len(self.instances)
         insts = (_lib.Instance * n)()
-        rows = {}  # psi0 rows by state_init object (instances often share the basis states)
-        dim_list = [dim_of[id(r[0])] for r in recs]
-        psi_rows = []
-        for k, r in enumerate(recs):
-            key = (id(r[5]), dim_list[k])
-            row = rows.get(key)
-            if row is None:
-                d = dim_list[k]
-                p = np.asarray(r[5], np.complex128).reshape(-1)
-                if p.size != d:
-                    raise ValueError(f"instance {k}: state_init must have {d} entries")
-                row = [0.0] * 6
-                row[0:2 * d:2] = p.real.tolist()
-                row[1:2 * d:2] = p.imag.tolist()
-                rows[key] = row
-            psi_rows.append(row)
-        times = np.array([r[1:5] for r in recs], np.float64).reshape(n, 4).T.copy()
-        t0, t1, dti, dto = times
-        psi0 = np.array(psi_rows, np.float64)
-        dims = np.array(dim_list, np.int32)
+        psi0 = np.ascontiguousarray(cols.psi0)
+        dims = np.ascontiguousarray(dims)
+        t0, t1, dti, dto = cols.times.T.copy()
         totals = (ctypes.c_int64 * 4)()
         _lib.check(lib.spinsim_batch_describe(n, t0.ctypes.data, t1.ctypes.data, dti.ctypes.data, dto.ctypes.data,
                                               dims.ctypes.data, psi0.ctypes.data, insts, totals))
         out_off, u_off, st_off, self.total_steps = (int(v) for v in totals)
         self._inst_np = np.frombuffer(insts, dtype=INSTANCE_DTYPE)
-        if any(getattr(i, "intervals", None) is not None for i in self.instances):
+        if cols.intervals.count(None) != n:
             out_off, u_off, st_off = self._restrict_to_pieces()
         keep = []
         params_host = []
@@ -171,6 +213,7 @@ class Batch:
             offs = np.cumsum([0] + sizes[:-1]).astype(np.int64)
             field_doubles = sum(sizes)
         # one device allocation, 256-byte aligned pieces
+        # time, U, state and spin come first and back to back: one host copy takes all of them
         pieces = {"time": 8 * max(1, out_off), "u": 8 * max(2, u_off), "state": 8 * max(2, st_off),
                   "spin": 24 * max(1, out_off), "workspace": ws_bytes, "fields": 8 * field_doubles}
         self.precision = Precision(precision)
@@ -345,6 +388,23 @@ class Batch:
         return self._spin
 
     @property
+    def output_bytes(self):
+        """Bytes from the start of the device block to the end of the spin piece: time, U, state and
+        spin, back to back (256-byte aligned pieces)."""
+        return self._offsets["workspace"]
+
+    def host_views(self, host):
+        """numpy (time, U, state, spin) views of a host copy of the first ``output_bytes`` of the
+        device block (a uint8 tensor or array), shaped like the device tensors."""
+        raw = host.numpy() if hasattr(host, "numpy") else np.asarray(host)
+        out = []
+        for name, dt in (("time", np.float64), ("u", np.complex128), ("state", np.complex128), ("spin", np.float64)):
+            o = self._offsets[name]
+            out.append(raw[o:o + self._pieces[name]].view(dt))
+        out[3] = out[3].reshape(-1, 3)
+        return out
+
+    @property
     def workspace(self):
         if "_workspace" not in self.__dict__:
             import torch
@@ -463,13 +523,15 @@ class Evaluator:
     """Evaluate lists of instances into host memory with the stages overlapped.
 
     The list is split into ``chunks`` contiguous groups of about equal work.  Group k's host set-up
-    (descriptors, field packing into pinned staging) and kernels run while group k-1's outputs are
-    copied to pinned host memory on a second stream, so the end-to-end time approaches the larger
-    of the kernel time and the device-to-host copy time instead of their sum.  ``evaluate`` returns
-    one ``Results`` per instance whose arrays are numpy views of page-locked host buffers.
-    Remaining keyword arguments go to ``Batch``; with ``lanes`` fixed and ``force_mixed=True`` the
-    results are bit-identical to one ``Batch`` of the whole list, otherwise a group may pick other
-    lanes or a single-spin kernel and the results agree to rounding.
+    (descriptors, field packing into pinned staging), uploads and kernels run while group k-1's
+    outputs are copied to pinned host memory, one copy per group; uploads, kernels and copies have
+    a stream each.  The copies are usually the longest stage (every output crosses PCIe), so the
+    end-to-end time approaches the time to set up and run the first group plus the time of all the
+    copies.  ``evaluate`` returns one ``Results`` per instance whose arrays are numpy views of
+    page-locked host buffers.  Remaining keyword arguments go to ``Batch``; with ``lanes``
+    fixed and ``force_mixed=True`` the results are bit-identical to one ``Batch`` of the whole
+    list, otherwise a group may pick other lanes or a single-spin kernel and the results agree to
+    rounding.
     """
 
     def __init__(self, chunks=6, **batch_kwargs):
@@ -479,6 +541,7 @@ class Evaluator:
         self.plans = batch_kwargs.pop("plan_cache", None)
         if self.plans is None:
             self.plans = {}
+        self.upload = torch.cuda.Stream()
         self.compute = torch.cuda.Stream()
         self.copy = torch.cuda.Stream()
         self.h2d_bytes = self.d2h_bytes = 0
@@ -489,18 +552,22 @@ class Evaluator:
         return torch.empty(max(256, int(nbytes)), dtype=torch.uint8, pin_memory=True)
 
     def groups(self, instances):
-        """Contiguous groups of about equal work (about (t1 - t0) / dt_int steps, spin one weighted
-        x8)."""
-        a = np.array([(i.time_start, i.time_end, i.time_step_integration, i.spin.dimension) for i in instances],
-                     np.float64).reshape(-1, 4)
-        work = np.maximum((a[:, 1] - a[:, 0]) / a[:, 2], 1.0) * np.where(a[:, 3] == 3, 8.0, 1.0)
+        """Contiguous (first, end) groups of about equal work (about (t1 - t0) / dt_int steps, spin
+        one weighted x8)."""
+        recs = list(map(_WORK_RECORD, instances))
+        n = len(recs)
+        if not n:
+            return []
+        a = np.fromiter(chain.from_iterable(map(itemgetter(0, 1, 2), recs)), np.float64, 3 * n).reshape(n, 3)
+        dims = _dims_of(_column(recs, 3))
+        work = np.maximum((a[:, 1] - a[:, 0]) / a[:, 2], 1.0) * np.where(dims == 3, 8.0, 1.0)
         cum = np.cumsum(work)
         cuts = [0]
         for g in range(1, self.chunks):
             k = int(np.searchsorted(cum, cum[-1] * g / self.chunks))
             if k > cuts[-1]:
                 cuts.append(k)
-        cuts.append(len(instances))
+        cuts.append(n)
         return [(a, b) for a, b in zip(cuts, cuts[1:]) if b > a]
 
     def evaluate(self, instances):
@@ -508,27 +575,32 @@ class Evaluator:
         instances = list(instances)
         if not instances:
             return []
-        keep, outs, self.h2d_bytes, self.d2h_bytes = [], [], 0, 0
+        outs, self.h2d_bytes, self.d2h_bytes = [], 0, 0
         for a, b in self.groups(instances):
-            stream = self.compute
-            with torch.cuda.stream(stream), torch.cuda.nvtx.range(f"spinsim.evaluate.group[{a}:{b}]"):
-                batch = Batch(instances[a:b], plan_cache=self.plans, staging=self._pinned, **self.kw)
-                batch.run()
-                done = torch.cuda.Event()
-                done.record(stream)
+            with torch.cuda.nvtx.range(f"spinsim.evaluate.group[{a}:{b}]"):
+                # Uploads on their own stream, so that they run during the previous group's kernels:
+                # small host-to-device copies are several times slower while a large device-to-host
+                # copy holds the link.
+                with torch.cuda.stream(self.upload):
+                    batch = Batch(instances[a:b], plan_cache=self.plans, staging=self._pinned, **self.kw)
+                    ready = torch.cuda.Event()
+                    ready.record(self.upload)
+                self.compute.wait_event(ready)
+                with torch.cuda.stream(self.compute):
+                    batch.run()
+                    done = torch.cuda.Event()
+                    done.record(self.compute)
             self.copy.wait_event(done)
-            host = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-                    for t in (batch.time, batch.u, batch.state, batch.spin)]
+            # time, U, state and spin lie back to back at the start of the batch's device block: one copy
+            nbytes = batch.output_bytes
+            host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
             with torch.cuda.stream(self.copy):
-                for h, t in zip(host, (batch.time, batch.u, batch.state, batch.spin)):
-                    h.copy_(t, non_blocking=True)
-            keep.append(batch)
-            outs.append((batch, [h.numpy() for h in host], host))
+                host.copy_(batch.memory[:nbytes], non_blocking=True)
+            outs.append((batch, host))
             self.h2d_bytes += batch.h2d_bytes
-            self.d2h_bytes += sum(h.numel() * h.element_size() for h in host)
+            self.d2h_bytes += nbytes
         self.copy.synchronize()
-        del keep
-        return HostResults([(batch._inst_np.copy(), arrays, host) for batch, arrays, host in outs])
+        return HostResults([(batch._inst_np.copy(), batch.host_views(host), host) for batch, host in outs])
 
 
 class HostResults:

@@ -12,6 +12,7 @@ is zero (``zero_boundary``) or the end value; the interval is found from the equ
 and then by bisection (I:2026-2061), so non-uniform tables work.
 """
 import math
+from operator import attrgetter, itemgetter, methodcaller
 
 import numpy as np
 
@@ -144,6 +145,7 @@ class ToneField(BuiltinField):
         if bias is not None:
             for c, v in (bias.items() if isinstance(bias, dict) else enumerate(bias)):
                 self.bias[_channel_index(c)] = v
+        self._cplan()  # the packing plan of the tone snapshots, made once here rather than at each launch
 
     def packed(self):
         """(flat (w, A, phi) array, start[8], count[8]), computed once (the tones are snapshots)."""
@@ -217,15 +219,22 @@ def _check_fields(fields):
         raise TypeError("packed fields must be built-in fields of one kind")
 
 
+_CPLAN = methodcaller("_cplan")
+_PLAN = attrgetter("_plan")  # set by the built-in fields' constructors
+
+
 def field_plan(fields):
     """The packing plan of a list of built-in fields of one kind (``spinsim_pack_fields`` rows) and
     the float64 entries the packed buffer takes, in one pass over the fields' cached plans."""
     _check_fields(fields)
     if not fields:
         return np.zeros((0, 8), np.int64), 0
-    cps = [f._cplan() for f in fields]
-    plan = np.concatenate([c[0] for c in cps]) if len(cps) > 1 else cps[0][0]
-    doubles = sum([c[1] for c in cps])
+    try:
+        cps = list(map(_PLAN, fields))
+    except AttributeError:
+        cps = list(map(_CPLAN, fields))
+    plan = np.concatenate(list(map(itemgetter(0), cps))) if len(cps) > 1 else cps[0][0]
+    doubles = sum(map(itemgetter(1), cps))
     if fields[0].kind == TabulatedField.kind:  # eight table descriptors per tabulated field
         doubles += 8 * _TABLE_DOUBLES * len(fields)
     return plan, doubles

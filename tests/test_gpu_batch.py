@@ -179,7 +179,9 @@ def test_evaluator_to_host_equals_batch(cuda, chunks):
     ev = B.Evaluator(chunks=chunks, lanes=1, force_mixed=True)
     res = ev.evaluate(insts)
     assert len(res) == len(insts)
-    assert ev.d2h_bytes == sum(t.numel() * t.element_size() for t in (ref.time, ref.u, ref.state, ref.spin))
+    # one copy per group of its time, U, state and spin pieces, with the alignment gaps between them
+    tensor_bytes = sum(t.numel() * t.element_size() for t in (ref.time, ref.u, ref.state, ref.spin))
+    assert tensor_bytes <= ev.d2h_bytes <= tensor_bytes + 3 * 256 * chunks
     for k in range(len(insts)):
         r = ref.result(k)
         for name in ("time", "time_evolution", "state", "spin"):
