@@ -549,15 +549,15 @@ def bench_serving(args):
                                  "admit_per_launch": 1e3 * srv.stats["host_admit_s"] / max(1, srv.stats["launches"]),
                                  "busy_fraction_of_span": (srv.stats["host_admit_s"] + srv.stats["host_complete_s"]) /
                                                           max(summ["span_s"], 1e-9)}})
-        return summ
+        return summ, srv.kw
 
     # capacity: the same mix with every request present at the start (the server saturated), and the
     # device alone: all of these requests as one batched launch, timed with CUDA events
     cap_reqs = synthetic_requests(args.requests, 1e12, seed=4)
-    capacity = serve(cap_reqs)
+    capacity, server_kw = serve(cap_reqs)
     steps_per_request = float(np.mean([r.steps() for r in cap_reqs]))
     from spinsim_b200.batch import Batch
-    one = Batch(cap_reqs, precision=ss.Precision.FP32_BULK, **kw)
+    one = Batch(cap_reqs, **server_kw)  # the server's kernel configuration
     device_s = _event_time(one.run)
     out["capacity"] = {"steps_per_s": capacity["steps_per_s"], "requests_per_s": capacity["steps_per_s"] / steps_per_request,
                        "mean_steps_per_request": steps_per_request, "launches": capacity["launches"],
@@ -567,7 +567,7 @@ def bench_serving(args):
                               "(device_steps_per_s: the same requests as one launch with state and spin)"}
     del one
     for rate in rates:
-        summ = serve(synthetic_requests(args.requests, rate, seed=4))
+        summ, _ = serve(synthetic_requests(args.requests, rate, seed=4))
         summ["offered_steps_per_s"] = rate * steps_per_request
         summ["load"] = rate * steps_per_request / capacity["steps_per_s"]  # above 1: latency grows with the backlog
         out["rates"][str(int(rate))] = summ
@@ -697,7 +697,7 @@ def main():
     ap.add_argument("--e2e-chunks", type=int, default=6, help="groups overlapped in the end-to-end measurement")
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=20000)
-    ap.add_argument("--streams", type=int, default=8)
+    ap.add_argument("--streams", type=int, default=4)
     ap.add_argument("--max-batch", type=int, default=2048)
     ap.add_argument("--max-steps-per-launch", type=float, default=0, help="serving: work cap of one launch")
     ap.add_argument("--hbm-budget-gb", type=float, default=16.0)
