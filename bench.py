@@ -654,10 +654,23 @@ def bench_configs(args):
 
 def profile_case(args):
     """One launch of the benchmark batch for profilers: the full batch, or a small case (the first 256
-    instances with durations capped at 1 ms) that a full ncu capture can replay quickly."""
+    instances with durations capped at 1 ms) that a full ncu capture can replay quickly.  With
+    ``--profile-field pulses``: one serving launch instead, ``--requests`` pulse-train requests of the
+    serving mix in the server's kernel configuration."""
     import torch
     import spinsim_b200 as ss
     from spinsim_b200.batch import Batch
+    if args.profile_field == "pulses":
+        from spinsim_b200.serving import Server, synthetic_requests
+        reqs = synthetic_requests(args.requests, 1e12, seed=4)
+        kw = Server(hbm_budget=1 << 20, warm_up=False).kw
+        if args.max_registers > 0:
+            kw["max_registers"] = args.max_registers
+        b = Batch(reqs, **kw)
+        b.run(with_state=not args.evolve_only)
+        torch.cuda.synchronize()
+        return {"workload": f"profile-pulses-{len(reqs)}", "precision": "fp32_bulk", "steps": b.total_steps,
+                "intervals": b.n_intervals, "plan": b.plan_info()}
     specs = workload()
     if args.profile_size == "small":
         specs = [(d, min(t, 1e-3), p) for d, t, p in specs[:256]]
@@ -686,6 +699,8 @@ def main():
     ap.add_argument("--workload", default="batch", choices=["batch", "serving", "configs", "profile"])
     ap.add_argument("--profile-size", default="small", choices=["small", "full"])
     ap.add_argument("--profile-spin", default="mixed", choices=["mixed", "half", "one"])
+    ap.add_argument("--profile-field", default="tones", choices=["tones", "pulses"],
+                    help="profile workload: the benchmark's tone batch, or one launch of serving requests")
     ap.add_argument("--precision", default="fp32_bulk", choices=["fp32_bulk", "fp64"])
     ap.add_argument("--max-registers", type=int, default=168)
     ap.add_argument("--lanes", type=int, default=0)

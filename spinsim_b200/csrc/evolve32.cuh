@@ -292,6 +292,77 @@ SS_D void su2_euler_step(Su2d& p, const double* g, float* nsq) {
 // in where a step samples the field and how it weights the samples: Magnus CF4 at the two Gauss
 // points with two exponentials (I:624-686), Heun at the step's ends with two half-step exponentials
 // (I:693-752), Euler at the midpoint with one exponential (I:759-791).
+// The state of interval32's step loop that the field samples need: the frame phasor W(t) =
+// exp(-i P rw (t - t_c)) advanced by an FP64 recurrence, its step and sample-offset factors, the
+// step start, the sample offsets and weights, and the table cursors.
+template <int L>
+struct Steps32 {
+    c64 W, Wrot, Woff;
+    double rw, t_fine, dt, off_a, off_b, c0, c1;
+    bool rotating;
+    TableCursor cur[L];
+};
+
+// One step's field samples (FP64) -> frame transform -> the integrator's generators (FP64); the
+// frame phasor moves on by one step.
+template <int FIELD, int L, int P, int INTEG>
+SS_D void step_generators32(const FieldDesc& f, Steps32<L>& st, double* ga, double* gb) {
+    double s0[8], s1[8];  // a user field writes all eight channels
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        s0[k] = 0.0;
+        s1[k] = 0.0;
+    }
+    sample_field<FIELD, L>(f, st.t_fine + st.off_a, s0, st.cur);
+    if (INTEG != INTEG_EULER) sample_field<FIELD, L>(f, st.t_fine + st.off_b, s1, st.cur);
+    if (st.rotating) {  // xy times exp(-i P rw tau), z minus P rw
+        const c64 Wn = st.W * st.Wrot;
+        const c64 xa = c64{s0[0], s0[1]} * (st.W * st.Woff);
+        s0[0] = xa.re;
+        s0[1] = xa.im;
+        s0[2] -= (double)P * st.rw;
+        if (INTEG != INTEG_EULER) {
+            const c64 xb = c64{s1[0], s1[1]} * (Wn * conj(st.Woff));
+            s1[0] = xb.re;
+            s1[1] = xb.im;
+            s1[2] -= (double)P * st.rw;
+        }
+        st.W = Wn;
+    }
+#pragma unroll
+    for (int k = 0; k < L; k++) {  // Euler: the one generator in ga (gb zero)
+        ga[k] = fma(st.c0, s0[k], st.c1 * s1[k]);
+        gb[k] = INTEG == INTEG_HEUN ? st.c0 * s1[k] : fma(st.c1, s0[k], st.c0 * s1[k]);
+    }
+}
+
+struct Generators4 {
+    double a[4], b[4];
+};
+
+struct SpinOneProduct {
+    Mat<3> u;
+    float nsq;
+};
+
+// Steps j .. j1-1 of a spin-one interval whose quadratic shift is non-zero: full 3x3 exponentials
+// and an FP64 3x3 product, from the product u of the steps before.  On entry st.t_fine is step j's
+// start and its generators are in g.  Out of line (and with its state passed by value), so that the
+// registers of the common SU(2) loop are allocated without this path's.
+template <int INTEG, int FIELD>
+__device__ __noinline__ SpinOneProduct spin_one_quadratic_steps32(const FieldDesc& f, Steps32<4> st, Mat<3> u,
+                                                                  Generators4 g, int j, int j1, float nsq) {
+    bool first = true;
+    for (; j < j1; j++) {
+        if (!first) step_generators32<FIELD, 4, 1, INTEG>(f, st, g.a, g.b);
+        first = false;
+        if constexpr (INTEG == INTEG_EULER) spin_one_euler_step(u, g.a, &nsq);
+        else spin_one_cf4_step(u, g.a, g.b, &nsq);
+        st.t_fine += st.dt;
+    }
+    return SpinOneProduct{u, nsq};
+}
+
 template <int D, int INTEG, int EXPO, int FIELD>
 SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDesc& f, int64_t index, bool active,
                      int lane_in_group, double* time_out, double* u_out, float* norms_out) {
@@ -301,14 +372,11 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     const int lanes = m.lanes;
     const double dt = inst.dt_int, dt_out = inst.dt_out;
     const double t_c = __dadd_rn(inst.t0, __dmul_rn(dt_out, (double)(inst.interval0 + index)));  // I:818, unfused
-    double s0[8], s1[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        s0[k] = 0.0;
-        s1[k] = 0.0;
-    }
     double rw = 0.0;
     if (active && m.rotating) {
+        double s0[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) s0[k] = 0.0;
         sample_field<FIELD, L>(f, t_c + dt_out / 2, s0);
         rw = s0[2];
         if (D == 2) rw /= 2;
@@ -330,45 +398,24 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
     const double c1 = INTEG == INTEG_CF4 ? dt * w1 : 0.0;
 
     // Frame phasor W(t) = exp(-i P rw (t - t_c)) by an FP64 recurrence, anchored at this lane's start.
-    c64 W = c64{1.0, 0.0}, Wrot = c64{1.0, 0.0}, Woff = c64{1.0, 0.0};
+    Steps32<L> st;
+    st.W = st.Wrot = st.Woff = c64{1.0, 0.0};
     if (m.rotating && K > 0) {
-        sincos(-(double)P * rw * (t_fine - t_c), &W.im, &W.re);
-        sincos(-(double)P * rw * dt, &Wrot.im, &Wrot.re);
-        sincos(-(double)P * rw * off_a, &Woff.im, &Woff.re);
+        sincos(-(double)P * rw * (t_fine - t_c), &st.W.im, &st.W.re);
+        sincos(-(double)P * rw * dt, &st.Wrot.im, &st.Wrot.re);
+        sincos(-(double)P * rw * off_a, &st.Woff.im, &st.Woff.re);
     }
-    TableCursor cur[L];  // per-channel table cursors for the increasing sample times of the steps
+    st.rw = rw;
+    st.t_fine = t_fine;
+    st.dt = dt;
+    st.off_a = off_a;
+    st.off_b = off_b;
+    st.c0 = c0;
+    st.c1 = c1;
+    st.rotating = m.rotating;
 #pragma unroll
-    for (int c = 0; c < L; c++) cur[c] = TableCursor{-1, 0.0, 0.0};
-
-    // One step's field samples (FP64) -> frame transform -> CF4 generators (FP64).
-    auto step_generators = [&](double* ga, double* gb) {
-#pragma unroll
-        for (int k = 0; k < L; k++) {
-            s0[k] = 0.0;
-            s1[k] = 0.0;
-        }
-        sample_field<FIELD, L>(f, t_fine + off_a, s0, cur);
-        if (INTEG != INTEG_EULER) sample_field<FIELD, L>(f, t_fine + off_b, s1, cur);
-        if (m.rotating) {  // xy times exp(-i P rw tau), z minus P rw
-            const c64 Wn = W * Wrot;
-            const c64 xa = c64{s0[0], s0[1]} * (W * Woff);
-            s0[0] = xa.re;
-            s0[1] = xa.im;
-            s0[2] -= (double)P * rw;
-            if (INTEG != INTEG_EULER) {
-                const c64 xb = c64{s1[0], s1[1]} * (Wn * conj(Woff));
-                s1[0] = xb.re;
-                s1[1] = xb.im;
-                s1[2] -= (double)P * rw;
-            }
-            W = Wn;
-        }
-#pragma unroll
-        for (int k = 0; k < L; k++) {  // Euler: the one generator in ga (gb zero)
-            ga[k] = fma(c0, s0[k], c1 * s1[k]);
-            gb[k] = INTEG == INTEG_HEUN ? c0 * s1[k] : fma(c1, s0[k], c0 * s1[k]);
-        }
-    };
+    for (int c = 0; c < L; c++) st.cur[c] = TableCursor{};  // for the increasing sample times of the steps
+    auto step_generators = [&](double* ga, double* gb) { step_generators32<FIELD, L, P, INTEG>(f, st, ga, gb); };
 
     // Phase 1: every step an SU(2) element (spin half always; spin one while the quadratic shift
     // is zero); the interval product is an FP64 SU(2) element.  Software-pipelined: the next step's
@@ -387,7 +434,7 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
             }
         }
         double na[4] = {0.0, 0.0, 0.0, 0.0}, nb[4] = {0.0, 0.0, 0.0, 0.0};
-        t_fine += dt;
+        st.t_fine += dt;
         if (j + 1 < j1) step_generators(na, nb);
         if constexpr (INTEG == INTEG_EULER) su2_euler_step(su2, ga, &nsq);
         else su2_cf4_step(su2, ga, gb, &nsq);
@@ -410,17 +457,18 @@ SS_D void interval32(const MethodConfig& m, const Instance& inst, const FieldDes
         }
     }
     // Phase 2 (spin one with a quadratic shift): full 3x3 exponentials and an FP64 3x3 product.
-    // On entry t_fine is the pending step's start and its generators are in ga, gb.
+    // On entry st.t_fine is the pending step's start and its generators are in ga, gb.
     if constexpr (D == 3) {
         if (pending) {
-            bool first = true;
-            for (; j < j1; j++) {
-                if (!first) step_generators(ga, gb);
-                first = false;
-                if constexpr (INTEG == INTEG_EULER) spin_one_euler_step(u, ga, &nsq);
-                else spin_one_cf4_step(u, ga, gb, &nsq);
-                t_fine += dt;
+            Generators4 g;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                g.a[k] = ga[k];
+                g.b[k] = gb[k];
             }
+            const SpinOneProduct r = spin_one_quadratic_steps32<INTEG, FIELD>(f, st, u, g, j, j1, nsq);
+            u = r.u;
+            nsq = r.nsq;
         }
     }
 

@@ -88,7 +88,7 @@ SS_D void interval64(const MethodConfig& m, const Instance& inst, const FieldDes
     set_identity(u);
     TableCursor cur[L];  // per-channel table cursors for the increasing sample times of the steps
 #pragma unroll
-    for (int c = 0; c < L; c++) cur[c] = TableCursor{-1, 0.0, 0.0};
+    for (int c = 0; c < L; c++) cur[c] = TableCursor{};
     const double a_lo = 0.5 * dt * (1.0 - 1.0 / kSqrt3);
     const double a_hi = 0.5 * dt * (1.0 + 1.0 / kSqrt3);
     const double w0 = (1.5 + kSqrt3) / 6.0, w1 = (1.5 - kSqrt3) / 6.0;

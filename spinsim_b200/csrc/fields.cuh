@@ -101,9 +101,16 @@ SS_D double table_sample(const TableChannel& tb, double ts) {
 // lands exactly on a table time (or outside the table) goes to the reference's search, which picks
 // among the touching intervals as the reference does.  Results are therefore identical to
 // table_sample; the cursor only removes the bisection's chain of dependent loads.
+//
+// A cursor also keeps the channel's value while it is constant on (t_lo, t_hi): a zero-order-hold
+// table's gain * amplitude[i] + bias, or the bias of a channel without a table (on the whole
+// line).  A sample strictly inside that interval then takes the kept value and reads no memory; it
+// is the value that the search would give there.
 struct TableCursor {
-    int64_t i;         // -1: not positioned
-    double t_lo, t_hi;
+    int32_t i = -1;    // -1: not positioned
+    int32_t hold = 0;  // 1: val is the channel's value on (t_lo, t_hi)
+    double t_lo = 0.0, t_hi = 0.0;
+    double val = 0.0;
 };
 
 SS_D double table_sample_cursor(const TableChannel& tb, double ts, TableCursor& cur) {
@@ -121,8 +128,8 @@ SS_D double table_sample_cursor(const TableChannel& tb, double ts, TableCursor& 
     }
     double u;
     const int64_t i = table_find(tb, ts, &u);
-    if (i >= 0 && i + 1 < tb.size) {
-        cur.i = i;
+    if (i >= 0 && i + 1 < tb.size && i < INT32_MAX) {
+        cur.i = (int32_t)i;
         cur.t_lo = __ldg(tb.time + i);
         cur.t_hi = __ldg(tb.time + i + 1);
     }
@@ -141,12 +148,29 @@ SS_D void sample_field(const FieldDesc& f, double t, double* out, TableCursor* c
     } else if constexpr (FIELD == FIELD_TABLE) {
 #pragma unroll
         for (int c = 0; c < NCH; c++) {
+            if (cursors && cursors[c].hold && t > cursors[c].t_lo && t < cursors[c].t_hi) {
+                out[c] = cursors[c].val;
+                continue;
+            }
             const TableChannel& tb = f.tables[c];
             if (tb.size > 0) {
                 const double v = cursors ? table_sample_cursor(tb, t, cursors[c]) : table_sample(tb, t);
                 out[c] = fma(f.gain[c], v, f.bias[c]);
+                if (cursors && tb.order == 0 && cursors[c].i >= 0) {
+                    TableCursor& cu = cursors[c];
+                    cu.hold = 1;
+                    cu.val = fma(f.gain[c], __ldg(tb.amplitude + cu.i), f.bias[c]);
+                }
             } else {
                 out[c] = f.bias[c];
+                if (cursors) {
+                    TableCursor& cu = cursors[c];
+                    cu.i = 0;
+                    cu.hold = 1;
+                    cu.t_lo = -INFINITY;
+                    cu.t_hi = INFINITY;
+                    cu.val = out[c];
+                }
             }
         }
     } else {  // FIELD_TONES
