@@ -240,7 +240,7 @@ class Server:
     one B200 for a mix of 10 us - 100 ms pulse-train requests near its capacity."""
 
     def __init__(self, precision=Precision.FP32_BULK, hbm_budget=8 << 30, streams=4, max_batch=4096,
-                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=80,
+                 copy_to_host=False, number_of_squares=24, threads_per_block=128, max_registers=128,
                  max_steps_per_launch=200_000_000, warm_up=True, staging_bytes=32 << 20):
         import torch
         self.precision = Precision(precision)
