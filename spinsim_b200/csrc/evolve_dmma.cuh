@@ -261,10 +261,6 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
             const double* lv = reinterpret_cast<const double*>(&lval[(c * kBulkTones + 2 * s + (q >> 1)) * kDmmaTile + row]);
             afr[c][s] = active ? lv[q & 1] : 0.0;
         }
-    double bias[3];  // (h / 2) bias
-#pragma unroll
-    for (int c = 0; c < 3; c++) bias[c] = half_dt * f.bias[c];
-
     // Rotating frame (I:823-829): Bz at the middle of the interval, sum_k Im(L_zk h_k) + bias;
     // lane q sums tones 2 q, 2 q + 1 and the quad adds the four parts.
     double rw = 0.0;
@@ -283,6 +279,12 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
     }
     const double prw = (double)P * rw;
     const double hprw = half_dt * prw;
+    // (h / 2) bias, the starting value of the samples' accumulation; in the rotating frame z also
+    // carries the frame's -P rw (I:582-618), added once here instead of to every sample
+    double bias[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) bias[c] = half_dt * f.bias[c];
+    bias[2] -= hprw;
     // Frame phasors at the Gauss points of this segment's steps: exp(-i P rw (tau - 0)), tau as above
     c64 wa = c64{1.0, 0.0}, wb = c64{1.0, 0.0}, wrot = c64{1.0, 0.0};
     if (m.rotating) {
@@ -345,15 +347,13 @@ SS_D void tile_dmma(const MethodConfig& m, const Instance& inst, const FieldDesc
                 sb[c] = nb[c];
             }
             if (active && m0 + mm < seg_len) {
-                if (m.rotating) {  // xy times exp(-i P rw tau), z minus P rw (I:582-618), in units of h / 2
+                if (m.rotating) {  // xy times exp(-i P rw tau) (I:582-618), in units of h / 2 (z: in the bias)
                     const c64 xa = c64{sa[0], sa[1]} * wa;
                     const c64 xb = c64{sb[0], sb[1]} * wb;
                     sa[0] = xa.re;
                     sa[1] = xa.im;
                     sb[0] = xb.re;
                     sb[1] = xb.im;
-                    sa[2] -= hprw;
-                    sb[2] -= hprw;
                     wa = wa * wrot;
                     wb = wb * wrot;
                 }
