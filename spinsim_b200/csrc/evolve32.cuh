@@ -252,8 +252,14 @@ SS_D void su2_apply_split(Su2d& p, double gx, double gy, double gz, const Su2f& 
     const c64 b = c64{fma(0.5, gy, (double)rest.beta.re), fma(-0.5, gx, (double)rest.beta.im)};
     // alpha' = alpha_e alpha - conj(beta_e) beta ; beta' = beta_e alpha + conj(alpha_e) beta
     const c64 alpha = c64{1.0 + p.am1.re, p.am1.im};
-    const c64 na = cfma(am1, alpha, p.am1) - conj(b) * p.beta;  // (alpha - 1) + am1 alpha - conj(b) beta
-    const c64 nb = cfma(b, alpha, cfma(conj(am1), p.beta, p.beta));
+    const c64 beta = p.beta;
+    // (alpha - 1) + am1 alpha - conj(b) beta and b alpha + conj(am1) beta + beta, each part one chain
+    // of four FMAs
+    c64 na, nb;
+    na.re = fma(-am1.im, alpha.im, fma(am1.re, alpha.re, fma(-b.im, beta.im, fma(-b.re, beta.re, p.am1.re))));
+    na.im = fma(am1.im, alpha.re, fma(am1.re, alpha.im, fma(b.im, beta.re, fma(-b.re, beta.im, p.am1.im))));
+    nb.re = fma(-b.im, alpha.im, fma(b.re, alpha.re, fma(am1.im, beta.im, fma(am1.re, beta.re, beta.re))));
+    nb.im = fma(b.im, alpha.re, fma(b.re, alpha.im, fma(-am1.im, beta.re, fma(am1.re, beta.im, beta.im))));
     p.am1 = na;
     p.beta = nb;
 }
