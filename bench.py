@@ -78,18 +78,19 @@ def instances(ss, specs):
 # products 128, time 1.  Spin one (Lie-Trotter, 24 squarings): field 192 + 48, windings 8 + 4,
 # frame 14, generators 32, two exponentials 10,920 + 14, two 3x3 products 432, time 1.  FP32-bulk
 # (tensor-path tone kernel, Magnus step): field samples 192 as FP64 tensor-core products (two Gauss
-# points x three channels x 16 multiply-adds) + the phasor table's recurrences 9, frame 26, sum and
+# points x three channels x 16 multiply-adds) + the phasor table's recurrences 9, frame 24 (the xy
+# rotations and the phasors' steps; z's frame shift is in the samples' starting value), sum and
 # difference of the samples 6, the exponential's linear part and the SU(2) product into the
 # interval's FP64 operator 39; in FP32 the commutator 15 and the exponential's O(|g|^2) remainder 21.
 # Spin one runs as SU(2) (no quadratic shift here).
 FLOPS_FP64_PLAIN = {2: 417 + 60, 3: 11600 + 66}
-FLOPS_BULK = {2: {"fp64": 272, "fp32": 36}, 3: {"fp64": 272, "fp32": 36}}
+FLOPS_BULK = {2: {"fp64": 270, "fp32": 36}, 3: {"fp64": 270, "fp32": 36}}
 # DRAM bytes (read + write) of one full-size FP32-bulk time-evolution launch of this workload (the
 # tensor-path kernel at 96 registers, writing the scan's tile partials and each output step's SU(2)
 # pair beside U: 46 MB of the writes are that scan scratch, not outputs), from one capture of
 # `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k regex:evolve_dmma -c 1`
 # on `bench.py --workload profile --profile-size full --precision fp32_bulk --max-registers 96 --variant 0`.
-TRAFFIC_BYTES_PER_LAUNCH = 7344384 + 139672320
+TRAFFIC_BYTES_PER_LAUNCH = 7328000 + 137223936
 
 
 def algorithmic_bytes(specs):
