@@ -710,7 +710,7 @@ def main():
     ap.add_argument("--bulk-config", default="",
                     help='FP32-bulk launch configuration as JSON (e.g. \'{"variant": 0, "max_registers": 96}\') '
                          "instead of autotuning it; for profiling runs, where serialised kernels distort the tuning")
-    ap.add_argument("--e2e-chunks", type=int, default=6, help="groups overlapped in the end-to-end measurement")
+    ap.add_argument("--e2e-chunks", type=int, default=8, help="groups overlapped in the end-to-end measurement")
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--streams", type=int, default=4)

@@ -46,7 +46,7 @@ INSTANCE_DTYPE = np.dtype(_lib.Instance)
 _INSTANCE_RECORD = attrgetter("spin", "time_start", "time_end", "time_step_integration", "time_step_output",
                               "state_init", "field")
 _TIMES = itemgetter(1, 2, 3, 4)
-_WORK_RECORD = attrgetter("time_start", "time_end", "time_step_integration", "spin")
+_GROUP_RECORD = attrgetter("time_start", "time_end", "time_step_output", "spin")
 
 
 def _column(records, k):
@@ -522,7 +522,7 @@ class Batch:
 class Evaluator:
     """Evaluate lists of instances into host memory with the stages overlapped.
 
-    The list is split into ``chunks`` contiguous groups of about equal work.  Group k's host set-up
+    The list is split into ``chunks`` contiguous groups of about equal output bytes.  Group k's host set-up
     (descriptors, field packing into pinned staging), uploads and kernels run while group k-1's
     outputs are copied to pinned host memory, one copy per group; uploads, kernels and copies have
     a stream each.  The copies are usually the longest stage (every output crosses PCIe), so the
@@ -534,7 +534,7 @@ class Evaluator:
     rounding.
     """
 
-    def __init__(self, chunks=6, **batch_kwargs):
+    def __init__(self, chunks=8, **batch_kwargs):
         import torch
         self.chunks = max(1, int(chunks))
         self.kw = batch_kwargs
@@ -552,15 +552,16 @@ class Evaluator:
         return torch.empty(max(256, int(nbytes)), dtype=torch.uint8, pin_memory=True)
 
     def groups(self, instances):
-        """Contiguous (first, end) groups of about equal work (about (t1 - t0) / dt_int steps, spin
-        one weighted x8)."""
-        recs = list(map(_WORK_RECORD, instances))
+        """Contiguous (first, end) groups of about equal output bytes, since the device-to-host copies
+        are the longest stage: about (t1 - t0) / dt_out output steps, spin one weighted 224 / 128 (the
+        bytes of time, U, state and spin per output step)."""
+        recs = list(map(_GROUP_RECORD, instances))
         n = len(recs)
         if not n:
             return []
         a = np.fromiter(chain.from_iterable(map(itemgetter(0, 1, 2), recs)), np.float64, 3 * n).reshape(n, 3)
         dims = _dims_of(_column(recs, 3))
-        work = np.maximum((a[:, 1] - a[:, 0]) / a[:, 2], 1.0) * np.where(dims == 3, 8.0, 1.0)
+        work = np.maximum((a[:, 1] - a[:, 0]) / a[:, 2], 1.0) * np.where(dims == 3, 224.0 / 128.0, 1.0)
         cum = np.cumsum(work)
         cuts = [0]
         for g in range(1, self.chunks):
@@ -632,7 +633,7 @@ class HostResults:
         return (self[i] for i in range(len(self)))
 
 
-def evaluate_many(instances, chunks=6, **batch_kwargs):
+def evaluate_many(instances, chunks=8, **batch_kwargs):
     """Evaluate a list of instances (see ``Instance``) into host ``Results`` with set-up, kernels
     and device-to-host copies overlapped across ``chunks`` groups (``Evaluator``)."""
     return Evaluator(chunks=chunks, **batch_kwargs).evaluate(instances)
