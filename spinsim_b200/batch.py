@@ -46,7 +46,7 @@ INSTANCE_DTYPE = np.dtype(_lib.Instance)
 _INSTANCE_RECORD = attrgetter("spin", "time_start", "time_end", "time_step_integration", "time_step_output",
                               "state_init", "field")
 _TIMES = itemgetter(1, 2, 3, 4)
-_GROUP_RECORD = attrgetter("time_start", "time_end", "time_step_output", "spin")
+_T0, _T1, _DT_OUT, _SPIN = (attrgetter(a) for a in ("time_start", "time_end", "time_step_output", "spin"))
 
 
 def _column(records, k):
@@ -555,13 +555,17 @@ class Evaluator:
         """Contiguous (first, end) groups of about equal output bytes, since the device-to-host copies
         are the longest stage: about (t1 - t0) / dt_out output steps, spin one weighted 224 / 128 (the
         bytes of time, U, state and spin per output step)."""
-        recs = list(map(_GROUP_RECORD, instances))
-        n = len(recs)
+        n = len(instances)
         if not n:
             return []
-        a = np.fromiter(chain.from_iterable(map(itemgetter(0, 1, 2), recs)), np.float64, 3 * n).reshape(n, 3)
-        dims = _dims_of(_column(recs, 3))
-        work = np.maximum((a[:, 1] - a[:, 0]) / a[:, 2], 1.0) * np.where(dims == 3, 224.0 / 128.0, 1.0)
+        t0 = np.fromiter(map(_T0, instances), np.float64, n)
+        t1 = np.fromiter(map(_T1, instances), np.float64, n)
+        dt_out = np.fromiter(map(_DT_OUT, instances), np.float64, n)
+        spins = list(map(_SPIN, instances))
+        ids = list(map(id, spins))
+        spin_one = {k for k, v in dict(zip(ids, spins)).items() if v.dimension == 3}  # few distinct objects
+        one = np.fromiter(map(spin_one.__contains__, ids), np.bool_, n)
+        work = np.maximum((t1 - t0) / dt_out, 1.0) * np.where(one, 224.0 / 128.0, 1.0)
         cum = np.cumsum(work)
         cuts = [0]
         for g in range(1, self.chunks):
